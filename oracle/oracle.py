@@ -1,0 +1,314 @@
+"""ctypes front-end of the CPU oracle (oracle/pf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, by ``__graft_entry__.smoke()`` as the checker
+and by ``bench.py`` for the CPU-baseline / reference arm.  The library under
+``pyfantom_b200`` never imports it.
+
+Every array argument is a numpy array (float64 / int32 / uint8); results are returned
+as new numpy arrays.  Grid conventions are those of the reference structured mesh
+(pyFANTOM/core/CUDA/Kernels/_geom.py:23-49); coarse operators are dense block
+stencils ``A[node, nb, dof, dof]`` with ``nb = (dx+1) + 3(dy+1) [+ 9(dz+1)]``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libpf_oracle.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_bp = ctypes.POINTER(ctypes.c_uint8)
+
+
+def build(force: bool = False) -> str:
+    """Compile pf_oracle.c with the system gcc (OpenMP) if needed; returns the .so path."""
+    src = os.path.join(_HERE, "pf_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        env = dict(os.environ)
+        env.pop("CC", None)
+        subprocess.run(["make", "-s", "-C", _HERE, "CC=gcc"], check=True, env=env)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        V = None
+        sigs = {
+            "or_matvec": (V, [ctypes.c_int, _ip, _dp, _dp, _dp, _bp, _dp]),
+            "or_diagonal": (V, [ctypes.c_int, _ip, _dp, _dp, _bp, _dp]),
+            "or_process_dk": (V, [ctypes.c_int, _ip, _dp, _dp, _dp]),
+            "or_restrict": (V, [ctypes.c_int, _ip, _dp, _dp]),
+            "or_prolong": (V, [ctypes.c_int, _ip, _dp, _dp]),
+            "or_galerkin_l0": (V, [ctypes.c_int, _ip, _dp, _dp, _bp, _dp]),
+            "or_galerkin_l1p": (V, [ctypes.c_int, _ip, _dp, _dp]),
+            "or_stencil_matvec": (V, [ctypes.c_int, _ip, _dp, _dp, _dp]),
+            "or_stencil_to_dense": (V, [ctypes.c_int, _ip, _dp, _dp]),
+            "or_cholesky": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_double, _dp]),
+            "or_cholesky_solve": (V, [ctypes.c_int, _dp, _dp, _dp]),
+            "or_mgcg_solve": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, _ip]),
+            "or_filter_normalizer": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp]),
+            "or_filter_fwd": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp]),
+            "or_filter_adj": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp, _dp]),
+            "or_oc_update": (ctypes.c_int, [ctypes.c_long, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp]),
+            "or_num_threads": (ctypes.c_int, []),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_ip)
+
+
+def _con(con, ndof):
+    if con is None:
+        return None, None
+    c = np.zeros(ndof, dtype=np.uint8)
+    con = np.asarray(con)
+    if con.dtype == bool and con.size == ndof:
+        c[:] = con
+    else:
+        c[con.astype(np.int64)] = 1
+    return c, c.ctypes.data_as(_bp)
+
+
+def n_nodes(nel):
+    return int(np.prod(np.asarray(nel) + 1))
+
+
+def n_elem(nel):
+    return int(np.prod(np.asarray(nel)))
+
+
+def coarse_nel(nel):
+    return tuple(int(n) // 2 for n in nel)
+
+
+def matvec(nel, K0, w, u, con=None):
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ua, pu = _d(u)
+    ca, pc = _con(con, nd)
+    out = np.zeros(nd)
+    lib().or_matvec(dim, pn, pK, pw, pu, pc, out.ctypes.data_as(_dp))
+    return out
+
+
+def diagonal(nel, K0, w, con=None):
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ca, pc = _con(con, nd)
+    out = np.zeros(nd)
+    lib().or_diagonal(dim, pn, pK, pw, pc, out.ctypes.data_as(_dp))
+    return out
+
+
+def process_dk(nel, K0, U):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    Ua, pU = _d(U)
+    out = np.zeros(n_elem(nel))
+    lib().or_process_dk(dim, pn, pK, pU, out.ctypes.data_as(_dp))
+    return out
+
+
+def restrict(nel, vf):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    va, pv = _d(vf)
+    out = np.zeros(n_nodes(coarse_nel(nel)) * dim)
+    lib().or_restrict(dim, pn, pv, out.ctypes.data_as(_dp))
+    return out
+
+
+def prolong(nel, vc):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    va, pv = _d(vc)
+    out = np.zeros(n_nodes(nel) * dim)
+    lib().or_prolong(dim, pn, pv, out.ctypes.data_as(_dp))
+    return out
+
+
+def _nb(dim):
+    return 27 if dim == 3 else 9
+
+
+def galerkin_l0(nel, K0, w, con=None):
+    """Level-1 block stencil from the fine operator (shape [n_coarse_nodes, nb, dof, dof])."""
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ca, pc = _con(con, nd)
+    out = np.zeros((n_nodes(coarse_nel(nel)), _nb(dim), dim, dim))
+    lib().or_galerkin_l0(dim, pn, pK, pw, pc, out.ctypes.data_as(_dp))
+    return out
+
+
+def galerkin_l1p(nel, A):
+    """Next-level block stencil from the level-(nel) stencil ``A``."""
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    Aa, pA = _d(A)
+    out = np.zeros((n_nodes(coarse_nel(nel)), _nb(dim), dim, dim))
+    lib().or_galerkin_l1p(dim, pn, pA, out.ctypes.data_as(_dp))
+    return out
+
+
+def stencil_matvec(nel, A, u):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    Aa, pA = _d(A)
+    ua, pu = _d(u)
+    out = np.zeros(n_nodes(nel) * dim)
+    lib().or_stencil_matvec(dim, pn, pA, pu, out.ctypes.data_as(_dp))
+    return out
+
+
+def stencil_to_dense(nel, A):
+    dim = len(nel)
+    N = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    Aa, pA = _d(A)
+    out = np.zeros((N, N))
+    lib().or_stencil_to_dense(dim, pn, pA, out.ctypes.data_as(_dp))
+    return out
+
+
+def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega=0.4, omega_boost=1.06,
+               tol=1e-8, maxiter=1000, x0=None):
+    """MultiGrid-preconditioned CG with the reference CUDA semantics.
+
+    Returns (x, iterations, relative recursive residual, status)."""
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ca, pc = _con(con, nd)
+    ra, pr = _d(rhs)
+    x = np.zeros(nd) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    res = ctypes.c_double(0.0)
+    st = ctypes.c_int(0)
+    it = lib().or_mgcg_solve(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
+                             pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None),
+                             ctypes.byref(res), ctypes.byref(st))
+    return x, int(it), float(res.value), int(st.value)
+
+
+def filter_weights(nel, h, r_min):
+    """Cone weights and integer offsets, restating geom/CUDA/_filters.py:65-98 (3D) and
+    the 2D twin: offsets over [-ceil(r), ceil(r)]^dim (meshgrid 'ij' order), distances
+    scaled by h/min(h), w = (r - d)/r kept where > 0, normalised to sum 1."""
+    dim = len(nel)
+    h = np.asarray(h, dtype=np.float64)
+    scales = h / h.min()
+    n = int(np.ceil(r_min))
+    rng = np.arange(-n, n + 1, dtype=np.int32)
+    grids = np.meshgrid(*([rng] * dim), indexing="ij")
+    offsets = np.vstack([g.ravel() for g in grids]).T
+    d = np.linalg.norm(offsets * scales[None], axis=1)
+    w = (r_min - d) / r_min
+    keep = w > 0
+    offsets, w = offsets[keep], w[keep]
+    w = w / w.sum()
+    return w.astype(np.float64), offsets.astype(np.int32)
+
+
+def filter_normalizer(nel, weights, offsets):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    wa, pw = _d(weights)
+    oa, po = _i(offsets)
+    out = np.zeros(n_elem(nel))
+    lib().or_filter_normalizer(dim, pn, len(wa), po, pw, out.ctypes.data_as(_dp))
+    return out
+
+
+def filter_fwd(nel, weights, offsets, v):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    wa, pw = _d(weights)
+    oa, po = _i(offsets)
+    va, pv = _d(v)
+    out = np.zeros(n_elem(nel))
+    lib().or_filter_fwd(dim, pn, len(wa), po, pw, pv, out.ctypes.data_as(_dp))
+    return out
+
+
+def filter_adj(nel, weights, offsets, normalizer, v):
+    dim = len(nel)
+    nel_a, pn = _i(nel)
+    wa, pw = _d(weights)
+    oa, po = _i(offsets)
+    na, pnm = _d(normalizer)
+    va, pv = _d(v)
+    out = np.zeros(n_elem(nel))
+    lib().or_filter_adj(dim, pn, len(wa), po, pw, pnm, pv, out.ctypes.data_as(_dp))
+    return out
+
+
+def oc_update(x, df, dg, vf, move):
+    """One OC step; returns (x_new, bisection steps)."""
+    xa, px = _d(x)
+    fa, pf = _d(df)
+    ga, pg = _d(np.broadcast_to(np.asarray(dg, dtype=np.float64), xa.shape))
+    out = np.zeros_like(xa)
+    steps = lib().or_oc_update(len(xa), px, pf, pg, float(vf), float(move), out.ctypes.data_as(_dp))
+    return out, int(steps)
+
+
+def penalize(rho, penalty=3.0, void=1e-9, E_mul=1.0, heavyside=False, beta=2.0, eta=0.5):
+    """SIMP law, Problem/CUDA/MinimumCompliance.py:305-324 (single material)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    if heavyside:
+        den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+        rho = (np.tanh(beta * eta) + np.tanh(beta * (rho - eta))) / den
+    e = np.clip(rho ** penalty, void, 1.0) * E_mul
+    return np.clip(e, void, None)
+
+
+def penalize_grad(rho, penalty=3.0, E_mul=1.0, heavyside=False, beta=2.0, eta=0.5):
+    """dE/drho without the clip term, Problem/CUDA/MinimumCompliance.py:351-367."""
+    rho = np.asarray(rho, dtype=np.float64)
+    if heavyside:
+        den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+        rh = (np.tanh(beta * eta) + np.tanh(beta * (rho - eta))) / den
+        df = penalty * rh ** (penalty - 1) * beta * (1 - np.tanh(beta * (rho - eta)) ** 2) / den
+    else:
+        df = penalty * rho ** (penalty - 1)
+    return df * E_mul
+
+
+def num_threads():
+    return int(lib().or_num_threads())
