@@ -1,0 +1,184 @@
+/*
+ * pyfantom_b200.h -- C ABI of the B200 (sm_100a) structured SIMP / MGCG library.
+ *
+ * The library replaces the CuPy RawModule kernels and launch wrappers of the reference
+ * pyFANTOM CUDA backend for structured Q4 / H8 meshes.  Every entry point returns an int
+ * status (PF_OK = 0); on failure pf_last_error() holds a message.  Pointers are DEVICE
+ * pointers unless the name starts with h_.  `stream` is a cudaStream_t passed as void*
+ * (NULL = legacy default stream).  No entry point allocates device memory except the
+ * *_create functions, which own what they allocate until the matching *_destroy.
+ *
+ * Layouts (reference pyFANTOM/core/CUDA/Kernels/_geom.py:23-49):
+ *   3D node (i,j,k) -> k + nz*(i + nx*j) ; element (i,j,k) -> (i*nely + j)*nelz + k
+ *   2D node (i,j)   -> i + nx*j          ; element (i,j)   -> i*nely + j
+ *   vectors are interleaved by DOF: v[node*dof + d]  (dof = dim)
+ *   node_mask: one uint8 per node, bit d set = DOF d is a Dirichlet DOF (NULL = none)
+ *   block stencils (coarse operators): structure-of-arrays
+ *     A[((nb*dof + a)*dof + b)*n_nodes + node], nb = (dx+1) + 3(dy+1) [+ 9(dz+1)],
+ *     i.e. the same 27 (3D) / 9 (2D) dof x dof blocks per row, in the same order, as the
+ *     reference's padded CSR (pyFANTOM/core/CUDA/Kernels/mgm.cu:384-395).
+ */
+#ifndef PYFANTOM_B200_H
+#define PYFANTOM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum pf_status {
+    PF_OK = 0,
+    PF_NOT_CONVERGED = 1, /* maxiter reached before the tolerance */
+    PF_BREAKDOWN = 2,     /* p.Kp <= 0 or r.z <= 0 in PCG (operator not SPD on the iterate) */
+    PF_NONFINITE = 3,     /* NaN / Inf found in an input or an iterate */
+    PF_TIMEOUT = 4,       /* a bounded device-side wait gave up */
+    PF_BAD_ARG = 5,       /* invalid argument (sizes, NULL pointers, unsupported options) */
+    PF_CUDA_ERROR = 6,    /* a CUDA runtime call failed */
+    PF_NO_MEMORY = 7,     /* device allocation failed */
+    PF_UNSUPPORTED = 8,   /* valid input the library does not handle (e.g. K0 without
+                             axis-reflection symmetry) */
+    PF_FACTOR_FAILED = 9  /* coarse Cholesky hit a non-positive pivot */
+};
+
+typedef struct pf_grid {
+    int dim;    /* 2 or 3 */
+    int nel[3]; /* elements along x, y, z (nel[2] ignored in 2D) */
+} pf_grid;
+
+/* ---- library ------------------------------------------------------------------------ */
+int pf_version(void);                     /* 100*major + minor */
+const char* pf_last_error(void);          /* message of the last failure on this thread */
+const char* pf_status_string(int status); /* static name of a status code */
+
+/* ---- element operator (replaces the K_single + node-incidence state of
+ *      pyFANTOM/stiffness/CUDA/_FEA.py:326-366) --------------------------------------- */
+typedef struct pf_op pf_op;
+/* h_K0: host row-major element matrix (24x24 for H8, 8x8 for Q4), DOF order (node, comp)
+ * with the reference local node order.  Fails with PF_UNSUPPORTED if K0 is not invariant
+ * under the element's axis reflections (the block structure the kernels rely on). */
+int pf_op_create(const pf_grid* grid, const double* h_K0, pf_op** out);
+int pf_op_destroy(pf_op* op);
+/* node mask from a per-DOF bool array (pyFANTOM/stiffness/CUDA/_FEA.py:441-456) */
+int pf_pack_mask(const pf_op* op, const uint8_t* con_dof, uint8_t* node_mask, void* stream);
+
+/* y = K(E) u with Dirichlet identity rows: y_c = u_c at constrained DOFs, constrained
+ * columns skipped.  Replaces mat_vec_node_basis_parallel[_wcon]_cuda_kernel
+ * (pyFANTOM/core/CUDA/Kernels/matvec.cu:1-98) behind StructuredStiffnessKernel._matvec
+ * (pyFANTOM/stiffness/CUDA/_FEA.py:518-549). */
+int pf_matvec_f64(const pf_op* op, const double* E, const double* u, const uint8_t* node_mask,
+                  double* y, void* stream);
+int pf_matvec_f32(const pf_op* op, const float* E, const float* u, const uint8_t* node_mask,
+                  float* y, void* stream);
+/* diag(K(E)), 1 at constrained DOFs.  Replaces get_diagonal_node_basis_cuda_kernel
+ * (diag.cu:1-47) behind StructuredStiffnessKernel.diagonal (_FEA.py:368-420). */
+int pf_diagonal_f64(const pf_op* op, const double* E, const uint8_t* node_mask, double* d,
+                    void* stream);
+/* dk_e = -u_e^T K0 u_e.  Replaces process_dk_kernel_cuda (grad.cu:1-16) behind
+ * StructuredStiffnessKernel.process_grad (_FEA.py:458-482). */
+int pf_sensitivity_f64(const pf_op* op, const double* U, double* dk, void* stream);
+
+/* ---- grid transfers (restriction_3d/2d_kernel, prolongation_3d/2d_kernel,
+ *      pyFANTOM/core/CUDA/Kernels/mgm.cu:1-244, via core/CUDA/_mgm.py:173-264) ---------- */
+/* `fine` is the fine grid; the coarse grid has nel/2 elements (nel must be even). */
+int pf_restrict_f64(const pf_grid* fine, const double* vf, double* vc, void* stream);
+int pf_prolong_f64(const pf_grid* fine, const double* vc, double* vf, void* stream);
+
+/* ---- Galerkin coarse operators (get_restricted_3d/2d_l0/l1p_nnz_based,
+ *      mgm.cu:247-895, via core/CUDA/_mgm.py:19-171) ---------------------------------- */
+int pf_galerkin_l0_f64(const pf_op* op, const double* E, const uint8_t* node_mask, double* A_coarse,
+                       void* stream);
+int pf_galerkin_l1p_f64(const pf_grid* fine, const double* A_fine, double* A_coarse, void* stream);
+int pf_stencil_matvec_f64(const pf_grid* grid, const double* A, const double* u, double* y,
+                          void* stream);
+size_t pf_stencil_size(const pf_grid* grid); /* doubles in one block stencil of `grid` */
+
+/* ---- multigrid-preconditioned CG (MultiGrid, pyFANTOM/solvers/CUDA/_solvers.py:330-660) */
+typedef struct pf_mg pf_mg;
+typedef struct pf_mg_config {
+    int n_level;        /* coarse levels below the fine grid (reference n_level) */
+    int n_smooth;       /* damped-Jacobi sweeps before and after the coarse correction */
+    double omega;       /* reference omega (max omega of the adaptive schedule) */
+    double min_omega;   /* reference min_omega argument (effective = max(omega/2, min_omega)) */
+    double omega_boost; /* omega growth per level (reference uses 1.06) */
+    double coarse_beta; /* diagonal shift of the coarse Cholesky (CHOLMOD beta = 1e-6) */
+    int precision;      /* 0 = FP64 V-cycle, 1 = FP32 V-cycle inside FP64 CG */
+    int check_every;    /* host convergence poll interval in iterations (>= 1) */
+} pf_mg_config;
+
+typedef struct pf_solve_info {
+    int iterations;     /* PCG iterations performed */
+    int status;         /* pf_status of the solve */
+    double residual;    /* ||r|| / ||b|| of the recursive residual at exit */
+    double setup_ms;    /* device time of the hierarchy setup inside this call */
+    double solve_ms;    /* device time of the iterations */
+} pf_solve_info;
+
+int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** out);
+int pf_mg_destroy(pf_mg* mg);
+/* Build D^-1, the Galerkin hierarchy and the coarse factor for densities E
+ * (MultiGrid._setup, _solvers.py:442-516). */
+int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask, void* stream);
+/* z = V-cycle(r) from a zero initial guess with Jacobi weight omega (MultiGrid._multi_grid,
+ * _solvers.py:518-571). */
+int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega, void* stream);
+/* PCG on K(E) x = b preconditioned by the V-cycle (MultiGrid.solve, _solvers.py:573-660).
+ * Requires pf_mg_setup.  use_x0 != 0 starts from the contents of x, else from 0.
+ * Blocks the calling thread until the solve ends; info is filled on return. */
+int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, int maxiter,
+                pf_solve_info* info, void* stream);
+/* Number of doubles of device workspace pf_cg_solve needs for `op`. */
+size_t pf_cg_workspace_size(const pf_op* op);
+/* Unpreconditioned CG on K(E) x = b (the matrix-free CG of _solvers.py:22-132).  `work`
+ * holds pf_cg_workspace_size(op) doubles. */
+int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node_mask, const double* b, double* x,
+                int use_x0, double tol, int maxiter, double* work, pf_solve_info* info, void* stream);
+
+/* ---- density filter (CuStructuredFilter2D/3D, pyFANTOM/geom/CUDA/_filters.py:14-201,
+ *      kernels filters.cu:1-154) ------------------------------------------------------ */
+typedef struct pf_filter pf_filter;
+/* h_offsets: n_taps x dim ints, h_weights: n_taps doubles (normalised to sum 1) */
+int pf_filter_create(const pf_grid* grid, int n_taps, const int* h_offsets, const double* h_weights,
+                     pf_filter** out);
+int pf_filter_destroy(pf_filter* f);
+int pf_filter_normalizer_f64(const pf_filter* f, double* out, void* stream);
+int pf_filter_fwd_f64(const pf_filter* f, const double* x, double* y, void* stream);
+int pf_filter_adj_f64(const pf_filter* f, const double* x, double* y, void* stream);
+
+/* ---- SIMP element-wise steps (MinimumCompliance.penalize / penalize_grad,
+ *      pyFANTOM/Problem/CUDA/MinimumCompliance.py:305-367) ----------------------------- */
+typedef struct pf_simp_params {
+    double penalty;
+    double void_value;
+    double E_mul;
+    double beta; /* Heaviside sharpness (used when heavyside != 0) */
+    double eta;  /* Heaviside threshold */
+    int heavyside;
+} pf_simp_params;
+/* E = penalize(rho); dE = penalize_grad(rho) (either output may be NULL) */
+int pf_penalize_f64(long long n, const double* rho, const pf_simp_params* p, double* E, double* dE,
+                    void* stream);
+/* out_e = dE_e * dk_e  (the element factor of the compliance sensitivity) */
+int pf_mul_f64(long long n, const double* a, const double* b, double* out, void* stream);
+
+/* ---- reductions --------------------------------------------------------------------- */
+size_t pf_dot_workspace_size(long long n); /* doubles */
+/* *result (device) = a . b, deterministic order; work holds pf_dot_workspace_size(n) doubles */
+int pf_dot_f64(long long n, const double* a, const double* b, double* result, double* work, void* stream);
+
+/* ---- OC update (Optimizers/CUDA/OC.py:67-144, single constraint) ---------------------- */
+size_t pf_oc_workspace_size(long long n); /* doubles */
+/* One OC step: ocP = x sqrt(max(-df/dg, 0)) (1e-3 everywhere if all zero), bisection on
+ * lambda in [1e-9, 1e9] until (l2-l1)/(l2+l1) <= 1e-8 testing dg.x_new - vf <= 0,
+ * x_new = max(0, max(x-move, min(1, min(x+move, ocP/lambda)))) (bounds clipped to [0,1]).
+ * h_out (host, may be NULL) receives {change = ||x_new - x||_2, lambda, steps}.
+ * work holds pf_oc_workspace_size(n) doubles. */
+int pf_oc_update_f64(long long n, const double* x, const double* df, const double* dg, double vf,
+                     double move, double* x_new, double* work, double* h_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYFANTOM_B200_H */

@@ -57,6 +57,8 @@ def lib():
             "or_mgcg_solve": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, _ip]),
+            "or_mg_vcycle": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, _dp, _dp, _bp, _dp, _dp]),
             "or_filter_normalizer": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp]),
             "or_filter_fwd": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp]),
             "or_filter_adj": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp, _dp]),
@@ -224,6 +226,22 @@ def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega
                              pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None),
                              ctypes.byref(res), ctypes.byref(st))
     return x, int(it), float(res.value), int(st.value)
+
+
+def mg_vcycle(nel, K0, w, con, r, n_level=3, n_smooth=2, omega=0.4, omega_boost=1.06):
+    """One V-cycle z = M r from a zero guess (level-0 Jacobi weight ``omega``)."""
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ca, pc = _con(con, nd)
+    ra, pr = _d(r)
+    z = np.zeros(nd)
+    st = lib().or_mg_vcycle(dim, pn, n_level, n_smooth, omega, omega_boost, pK, pw, pc, pr, z.ctypes.data_as(_dp))
+    if st:
+        raise RuntimeError(f"coarse Cholesky failed at pivot {st}")
+    return z
 
 
 def filter_weights(nel, h, r_min):

@@ -536,6 +536,64 @@ static double dot(long n, const double* a, const double* b) {
     return s;
 }
 
+static int mg_build(mg_t* m, int dim, const int* nel, int n_level, int n_smooth, double omega_boost,
+                    const double* K0, const double* w, const uint8_t* con) {
+    memset(m, 0, sizeof(*m));
+    m->dim = dim;
+    m->n_level = n_level;
+    m->n_smooth = n_smooth;
+    m->K0 = K0;
+    m->w = w;
+    m->con = con;
+    m->omega_boost = omega_boost;
+    for (int l = 0; l <= n_level; l++) {
+        for (int a = 0; a < dim; a++) m->nel[l][a] = nel[a] >> l;
+        grid_t g = mkgrid(dim, m->nel[l]);
+        m->ndof[l] = g.n_nodes * dim;
+        for (int t = 0; t < 5; t++) m->tmp[l][t] = (double*)calloc(m->ndof[l], sizeof(double));
+        m->Dinv[l] = (double*)malloc(sizeof(double) * m->ndof[l]);
+    }
+    /* setup (_solvers.py:442-496) */
+    or_diagonal(dim, m->nel[0], K0, w, con, m->Dinv[0]);
+    for (long i = 0; i < m->ndof[0]; i++) m->Dinv[0][i] = 1.0 / m->Dinv[0][i];
+    const int NB = n_blocks(dim), bs = dim * dim;
+    for (int l = 1; l <= n_level; l++) {
+        m->A[l] = (double*)malloc(sizeof(double) * (m->ndof[l] / dim) * NB * bs);
+        if (l == 1)
+            or_galerkin_l0(dim, m->nel[0], K0, w, con, m->A[1]);
+        else
+            or_galerkin_l1p(dim, m->nel[l - 1], m->A[l - 1], m->A[l]);
+        or_stencil_diagonal(dim, m->nel[l], m->A[l], m->Dinv[l]);
+        for (long i = 0; i < m->ndof[l]; i++) m->Dinv[l][i] = 1.0 / m->Dinv[l][i];
+    }
+    long nc = m->ndof[n_level];
+    double* dense = (double*)malloc(sizeof(double) * nc * nc);
+    m->Lc = (double*)malloc(sizeof(double) * nc * nc);
+    or_stencil_to_dense(dim, m->nel[n_level], m->A[n_level], dense);
+    int st = or_cholesky((int)nc, dense, 1e-6, m->Lc);
+    free(dense);
+    return st;
+}
+
+static void mg_release(mg_t* m) {
+    for (int l = 0; l <= m->n_level; l++) {
+        for (int t = 0; t < 5; t++) free(m->tmp[l][t]);
+        free(m->Dinv[l]);
+        if (l) free(m->A[l]);
+    }
+    free(m->Lc);
+}
+
+/* One V-cycle z = M r from a zero guess with level-0 Jacobi weight omega. */
+int or_mg_vcycle(int dim, const int* nel, int n_level, int n_smooth, double omega, double omega_boost,
+                 const double* K0, const double* w, const uint8_t* con, const double* r, double* z) {
+    mg_t m;
+    int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con);
+    if (st == 0) vcycle(&m, 0, z, r, omega);
+    mg_release(&m);
+    return st;
+}
+
 /* returns iterations; *res = final recursive relative residual; status 0 ok, 1 not
  * converged, 2 coarse factorization failed */
 int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
@@ -543,40 +601,7 @@ int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double ome
                   const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
                   int* status_out) {
     mg_t m;
-    memset(&m, 0, sizeof(m));
-    m.dim = dim;
-    m.n_level = n_level;
-    m.n_smooth = n_smooth;
-    m.K0 = K0;
-    m.w = w;
-    m.con = con;
-    m.omega_boost = omega_boost;
-    for (int l = 0; l <= n_level; l++) {
-        for (int a = 0; a < dim; a++) m.nel[l][a] = nel[a] >> l;
-        grid_t g = mkgrid(dim, m.nel[l]);
-        m.ndof[l] = g.n_nodes * dim;
-        for (int t = 0; t < 5; t++) m.tmp[l][t] = (double*)calloc(m.ndof[l], sizeof(double));
-        m.Dinv[l] = (double*)malloc(sizeof(double) * m.ndof[l]);
-    }
-    /* setup (_solvers.py:442-496) */
-    or_diagonal(dim, m.nel[0], K0, w, con, m.Dinv[0]);
-    for (long i = 0; i < m.ndof[0]; i++) m.Dinv[0][i] = 1.0 / m.Dinv[0][i];
-    const int NB = n_blocks(dim), bs = dim * dim;
-    for (int l = 1; l <= n_level; l++) {
-        m.A[l] = (double*)malloc(sizeof(double) * (m.ndof[l] / dim) * NB * bs);
-        if (l == 1)
-            or_galerkin_l0(dim, m.nel[0], K0, w, con, m.A[1]);
-        else
-            or_galerkin_l1p(dim, m.nel[l - 1], m.A[l - 1], m.A[l]);
-        or_stencil_diagonal(dim, m.nel[l], m.A[l], m.Dinv[l]);
-        for (long i = 0; i < m.ndof[l]; i++) m.Dinv[l][i] = 1.0 / m.Dinv[l][i];
-    }
-    long nc = m.ndof[n_level];
-    double* dense = (double*)malloc(sizeof(double) * nc * nc);
-    m.Lc = (double*)malloc(sizeof(double) * nc * nc);
-    or_stencil_to_dense(dim, m.nel[n_level], m.A[n_level], dense);
-    int st = or_cholesky((int)nc, dense, 1e-6, m.Lc);
-    free(dense);
+    int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con);
     int iters = 0;
     double R = 0.0;
     int status = 0;
@@ -621,12 +646,7 @@ int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double ome
         }
         free(r); free(z); free(p); free(q);
     }
-    for (int l = 0; l <= n_level; l++) {
-        for (int t = 0; t < 5; t++) free(m.tmp[l][t]);
-        free(m.Dinv[l]);
-        if (l) free(m.A[l]);
-    }
-    free(m.Lc);
+    mg_release(&m);
     *res_out = R;
     *status_out = status;
     return iters;

@@ -1,0 +1,525 @@
+// Element operator of the structured SIMP stiffness K(E) = sum_e E_e K0_e:
+// matvec (with Dirichlet identity rows), diagonal and -u_e^T K0 u_e.
+//
+// H8 factorisation.  Both axis-aligned reflections of a box element map the element onto
+// itself, so K0 commutes with them.  In the Walsh basis of the 2x2x2 corners
+// (v = T u with T[(m,c),(l,c')] = delta_cc' prod_axis (m_axis ? +-1 : 1)) K0 becomes
+// block diagonal: B = T K0 T^T / 64 has eight 3x3 blocks, one per parity class
+// p = (px,py,pz), coupling component c in mode p ^ e_c.  K0 u = T^T B T u costs
+// 3 butterfly stages forward, 8 3x3 blocks and 3 stages back (~190 flops, against 576
+// multiply-adds for the dense 24x24 product).  The matvec kernel marches along x: warps
+// cover element rows in y, lanes cover element columns in z (the contiguous node axis),
+// so every plane of nodal values is read once, coalesced, into shared memory; the forward
+// and inverse y/z stages are done once per face and shared by the two elements on either
+// side of it; node sums across the tile use warp shuffles and one shared-memory exchange.
+// Owner-computes: each node of the tile is written once, no atomics, fixed summation order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "elemop.cuh"
+
+namespace pf {
+
+// ---------------------------------------------------------------------------------------
+// host: transform-block factorisation of K0
+// ---------------------------------------------------------------------------------------
+static const int kCX[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+static const int kCY[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+static const int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+
+static int walsh(int m, int l, int dim) {
+    int pos[3] = {kCX[l], kCY[l], dim == 3 ? kCZ[l] : 0};
+    int s = 1;
+    for (int a = 0; a < dim; a++)
+        if ((m >> a) & 1) s *= pos[a] ? 1 : -1;
+    return s;
+}
+
+int op_factorise(Op* op) {
+    const int dim = op->grid.dim, nc = dim == 3 ? 8 : 4, nd = nc * dim;
+    // T (nd x nd): row (m, c), column (l, c')
+    std::vector<double> T(nd * nd, 0.0), tmp(nd * nd, 0.0), B(nd * nd, 0.0);
+    for (int m = 0; m < nc; m++)
+        for (int l = 0; l < nc; l++)
+            for (int c = 0; c < dim; c++) T[(m * dim + c) * nd + l * dim + c] = walsh(m, l, dim);
+    // B = T K0 T^T / nc^2
+    for (int i = 0; i < nd; i++)
+        for (int j = 0; j < nd; j++) {
+            double s = 0;
+            for (int k = 0; k < nd; k++) s += T[i * nd + k] * op->K0[k * nd + j];
+            tmp[i * nd + j] = s;
+        }
+    double bmax = 0.0;
+    for (int i = 0; i < nd; i++)
+        for (int j = 0; j < nd; j++) {
+            double s = 0;
+            for (int k = 0; k < nd; k++) s += tmp[i * nd + k] * T[j * nd + k];
+            B[i * nd + j] = s / double(nc * nc);
+            bmax = fmax(bmax, fabs(B[i * nd + j]));
+        }
+    // extract class blocks and verify that nothing lies outside them
+    std::vector<char> used(nd * nd, 0);
+    for (int p = 0; p < nc; p++)
+        for (int c = 0; c < dim; c++)
+            for (int c2 = 0; c2 < dim; c2++) {
+                int row = (p ^ (1 << c)) * dim + c, col = (p ^ (1 << c2)) * dim + c2;
+                op->blk[p][c][c2] = B[row * nd + col];
+                used[row * nd + col] = 1;
+            }
+    double off = 0.0;
+    for (int i = 0; i < nd * nd; i++)
+        if (!used[i]) off = fmax(off, fabs(B[i]));
+    if (!(off <= 1e-12 * bmax))
+        return fail(PF_UNSUPPORTED,
+                    "K0 is not invariant under the element's axis reflections (off-block %.3e vs %.3e)", off, bmax);
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// 3D matvec: x-marching tile kernel
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct H8Blk {
+    T b[8][3][3];
+};
+
+template <typename T, typename TE, int TY>
+__global__ void __launch_bounds__((TY + 1) * 32)
+    k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
+                const uint8_t* __restrict__ mask, const H8Blk<T> blk, Epi<T> epi) {
+    constexpr int NW = TY + 1;
+    constexpr int NT = NW * 32;
+    constexpr int PR = TY + 2, PC = 33;
+    __shared__ T s_u[2][3][PR][PC];
+    __shared__ T s_x[3][NW][32];
+    __shared__ double s_red[NW];
+
+    if (epi.skip && *epi.skip) return;
+    const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int kz0 = blockIdx.x * 31, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
+    const int je = jy0 - 1 + w, ke = kz0 - 1 + l;
+    const int jn = jy0 + w, kn = kz0 + l;
+    const bool owner = (w < TY) && (l < 31) && (jn < ny) && (kn < nz);
+    const bool col_ok = (je >= 0) && (je < NY) && (ke >= 0) && (ke < NZ);
+    const T wgt = epi_omega(epi);
+    double dot = 0.0;
+
+    auto load_plane = [&](int p, int buf) {
+        for (int idx = threadIdx.x; idx < PR * PC; idx += NT) {
+            const int r = idx / PC, c = idx - r * PC;
+            const int j = jy0 - 1 + r, k = kz0 - 1 + c;
+            T v0 = T(0), v1 = T(0), v2 = T(0);
+            if (p >= 0 && p < nx && j >= 0 && j < ny && k >= 0 && k < nz) {
+                const long long n = (long long)k + (long long)nz * (p + (long long)nx * j);
+                const uint8_t m = mask ? mask[n] : (uint8_t)0;
+                v0 = (m & 1) ? T(0) : u[3 * n];
+                v1 = (m & 2) ? T(0) : u[3 * n + 1];
+                v2 = (m & 4) ? T(0) : u[3 * n + 2];
+            }
+            s_u[buf][0][r][c] = v0;
+            s_u[buf][1][r][c] = v1;
+            s_u[buf][2][r][c] = v2;
+        }
+    };
+    // forward y/z stages on this thread's face: g[comp][mb][mc]
+    auto face = [&](int buf, T g[3][2][2]) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const T f00 = s_u[buf][c][w][l], f01 = s_u[buf][c][w][l + 1];
+            const T f10 = s_u[buf][c][w + 1][l], f11 = s_u[buf][c][w + 1][l + 1];
+            const T s0 = f00 + f10, s1 = f01 + f11, d0 = f10 - f00, d1 = f11 - f01;
+            g[c][0][0] = s0 + s1;
+            g[c][0][1] = s1 - s0;
+            g[c][1][0] = d0 + d1;
+            g[c][1][1] = d1 - d0;
+        }
+    };
+
+    load_plane(ix0 - 1, 0);
+    __syncthreads();
+    T glo[3][2][2], carry[3][2][2];
+    face(0, glo);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) carry[c][a][b] = T(0);
+
+    int buf = 0;
+    for (int s = 0; s <= CXc; s++) {
+        const int ie = ix0 - 1 + s;
+        const int nb = buf ^ 1;
+        load_plane(ie + 1, nb);
+        __syncthreads();
+        T ghi[3][2][2];
+        face(nb, ghi);
+        T e = T(0);
+        if (col_ok && ie >= 0 && ie < NX) e = (T)E[((long long)ie * NY + je) * NZ + ke];
+        // x stage (with the density folded in): v[c][ma][mb][mc]
+        T v[3][2][2][2];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int mb = 0; mb < 2; mb++)
+#pragma unroll
+                for (int mc = 0; mc < 2; mc++) {
+                    const T t = e * ghi[c][mb][mc];
+                    v[c][0][mb][mc] = fma(e, glo[c][mb][mc], t);
+                    v[c][1][mb][mc] = fma(-e, glo[c][mb][mc], t);
+                }
+        // class blocks: component c of class p sits in mode p ^ e_c
+        T wv[3][2][2][2];
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            const int px = p & 1, py = (p >> 1) & 1, pz = (p >> 2) & 1;
+            const T i0 = v[0][px ^ 1][py][pz], i1 = v[1][px][py ^ 1][pz], i2 = v[2][px][py][pz ^ 1];
+            wv[0][px ^ 1][py][pz] = fma(blk.b[p][0][0], i0, fma(blk.b[p][0][1], i1, blk.b[p][0][2] * i2));
+            wv[1][px][py ^ 1][pz] = fma(blk.b[p][1][0], i0, fma(blk.b[p][1][1], i1, blk.b[p][1][2] * i2));
+            wv[2][px][py][pz ^ 1] = fma(blk.b[p][2][0], i0, fma(blk.b[p][2][1], i1, blk.b[p][2][2] * i2));
+        }
+        // inverse x stage; the lower face completes with the previous layer's upper face
+        T t[3][2][2];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            T G[2][2];
+#pragma unroll
+            for (int mb = 0; mb < 2; mb++)
+#pragma unroll
+                for (int mc = 0; mc < 2; mc++) {
+                    const T w0 = wv[c][0][mb][mc], w1 = wv[c][1][mb][mc];
+                    G[mb][mc] = (w0 - w1) + carry[c][mb][mc];
+                    carry[c][mb][mc] = w0 + w1;
+                }
+            // inverse z then y stage -> corner contributions t[c][b][cz]
+            const T q00 = G[0][0] - G[0][1], q01 = G[0][0] + G[0][1];
+            const T q10 = G[1][0] - G[1][1], q11 = G[1][0] + G[1][1];
+            t[c][0][0] = q00 - q10;
+            t[c][0][1] = q01 - q11;
+            t[c][1][0] = q00 + q10;
+            t[c][1][1] = q01 + q11;
+        }
+        // node (je+1, ke+1) = t_own[1][1] + t_{l+1}[1][0] + t_{w+1}[0][1] + t_{w+1,l+1}[0][0]
+        T P1[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            P1[c] = t[c][1][1] + __shfl_down_sync(0xffffffffu, t[c][1][0], 1);
+            const T P0 = t[c][0][1] + __shfl_down_sync(0xffffffffu, t[c][0][0], 1);
+            s_x[c][w][l] = P0;
+        }
+        __syncthreads();
+        if (owner && s >= 1 && ie < nx) {
+            const long long n = (long long)kn + (long long)nz * (ie + (long long)nx * jn);
+            const uint8_t m = mask ? mask[n] : (uint8_t)0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                T y = P1[c] + s_x[c][w + 1][l];
+                if (m & (1 << c)) y = u[3 * n + c];
+                const long long g = 3 * n + c;
+                const T o = epi_apply(epi, g, y, wgt);
+                epi.out[g] = o;
+                if (epi.dot_partial) dot += (double)epi.dot_a[g] * (double)(epi.dot_of_y ? y : o);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int b = 0; b < 2; b++) glo[c][a][b] = ghi[c][a][b];
+        buf = nb;
+    }
+    if (epi.dot_partial) {
+        const double sblk = block_sum<NT>(dot, s_red);
+        if (threadIdx.x == 0)
+            epi.dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = sblk;
+    }
+}
+
+template <typename T>
+static H8Blk<T> make_blk(const Op* op) {
+    H8Blk<T> b;
+    for (int p = 0; p < 8; p++)
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) b.b[p][i][j] = (T)op->blk[p][i][j];
+    return b;
+}
+
+constexpr int kTY64 = 4;  // FP64: 5 warps per block
+constexpr int kTY32 = 8;  // FP32: 9 warps per block
+
+static void h8_launch_dims(const Grid& g, int TY, dim3* grid, int* CXc) {
+    const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
+    const int tz = (nz + 30) / 31, ty = (ny + TY - 1) / TY;
+    // enough x-chunks for ~4 waves of blocks, chunks of 4..32 planes
+    const long long target = 4LL * kNumSM * 3;
+    int chunks = (int)((target + (long long)tz * ty - 1) / ((long long)tz * ty));
+    int cx = (nx + chunks - 1) / chunks;
+    cx = cx < 4 ? 4 : (cx > 32 ? 32 : cx);
+    *CXc = cx;
+    *grid = dim3(tz, ty, (nx + cx - 1) / cx);
+}
+
+long long h8_num_blocks(const Grid& g, int fp32) {
+    dim3 gr;
+    int cx;
+    h8_launch_dims(g, fp32 ? kTY32 : kTY64, &gr, &cx);
+    return (long long)gr.x * gr.y * gr.z;
+}
+
+// ---------------------------------------------------------------------------------------
+// 2D matvec (node gather, dense 8x8 K0)
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct Q4K {
+    T k[8][8];
+};
+
+template <typename T, typename TE>
+__global__ void __launch_bounds__(256) k_matvec_q4(int NX, int NY, const T* __restrict__ u, const TE* __restrict__ E,
+                                                   const uint8_t* __restrict__ mask, const Q4K<T> K, Epi<T> epi) {
+    __shared__ double s_red[8];
+    if (epi.skip && *epi.skip) return;
+    const int nx = NX + 1, ny = NY + 1;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dot = 0.0;
+    const T wgt = epi_omega(epi);
+    if (n < (long long)nx * ny) {
+        const int i = (int)(n % nx), j = (int)(n / nx);
+        const uint8_t mn = mask ? mask[n] : (uint8_t)0;
+        T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int ei = i - kCXd(r), ej = j - kCYd(r);
+            if (ei < 0 || ej < 0 || ei >= NX || ej >= NY) continue;
+            const T we = (T)E[(long long)ei * NY + ej];
+            T a0 = T(0), a1 = T(0);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const long long m = (long long)(ei + kCXd(q)) + (long long)nx * (ej + kCYd(q));
+                const uint8_t mm = mask ? mask[m] : (uint8_t)0;
+                const T u0 = (mm & 1) ? T(0) : u[2 * m], u1 = (mm & 2) ? T(0) : u[2 * m + 1];
+                a0 = fma(K.k[2 * r][2 * q], u0, fma(K.k[2 * r][2 * q + 1], u1, a0));
+                a1 = fma(K.k[2 * r + 1][2 * q], u0, fma(K.k[2 * r + 1][2 * q + 1], u1, a1));
+            }
+            acc0 = fma(a0, we, acc0);
+            acc1 = fma(a1, we, acc1);
+        }
+        T y[2] = {acc0, acc1};
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            if (mn & (1 << c)) y[c] = u[2 * n + c];
+            const long long g = 2 * n + c;
+            const T o = epi_apply(epi, g, y[c], wgt);
+            epi.out[g] = o;
+            if (epi.dot_partial) dot += (double)epi.dot_a[g] * (double)(epi.dot_of_y ? y[c] : o);
+        }
+    }
+    if (epi.dot_partial) {
+        const double sblk = block_sum<256>(dot, s_red);
+        if (threadIdx.x == 0) epi.dot_partial[blockIdx.x] = sblk;
+    }
+}
+
+template <typename T>
+static Q4K<T> make_q4k(const Op* op) {
+    Q4K<T> K;
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++) K.k[i][j] = (T)op->K0[i * 8 + j];
+    return K;
+}
+
+long long q4_num_blocks(const Grid& g) { return (g.n_nodes + 255) / 256; }
+
+// ---------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------
+template <typename T, typename TE>
+int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mask, const Epi<T>& epi,
+                       cudaStream_t st) {
+    const Grid& g = op->grid;
+    if (g.dim == 3) {
+        constexpr int TY = sizeof(T) == 8 ? kTY64 : kTY32;
+        dim3 grid;
+        int cx;
+        h8_launch_dims(g, TY, &grid, &cx);
+        k_matvec_h8<T, TE, TY><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
+                                                             make_blk<T>(op), epi);
+    } else {
+        const long long nb = q4_num_blocks(g);
+        k_matvec_q4<T, TE><<<(unsigned)nb, 256, 0, st>>>(g.nel[0], g.nel[1], u, E, mask, make_q4k<T>(op), epi);
+    }
+    PF_LAUNCH_CHECK("fine matvec launch");
+    return PF_OK;
+}
+
+long long fine_matvec_num_blocks(const Op* op, int fp32) {
+    return op->grid.dim == 3 ? h8_num_blocks(op->grid, fp32) : q4_num_blocks(op->grid);
+}
+
+template int launch_fine_matvec<double, double>(const Op*, const double*, const double*, const uint8_t*,
+                                                const Epi<double>&, cudaStream_t);
+template int launch_fine_matvec<float, float>(const Op*, const float*, const float*, const uint8_t*,
+                                              const Epi<float>&, cudaStream_t);
+
+// ---------------------------------------------------------------------------------------
+// diagonal, sensitivity, mask packing
+// ---------------------------------------------------------------------------------------
+struct KDiag {
+    double d[24];
+};
+
+template <typename T>
+__global__ void k_diagonal(Grid g, const double* __restrict__ E, const uint8_t* __restrict__ mask, KDiag kd,
+                           T* __restrict__ diag) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.n_nodes) return;
+    const int dof = g.dim, nc = g.dim == 3 ? 8 : 4;
+    int i, j, k;
+    if (g.dim == 3) {
+        k = (int)(n % g.nn[2]);
+        const long long t = n / g.nn[2];
+        i = (int)(t % g.nn[0]);
+        j = (int)(t / g.nn[0]);
+    } else {
+        i = (int)(n % g.nn[0]);
+        j = (int)(n / g.nn[0]);
+        k = 0;
+    }
+    const uint8_t m = mask ? mask[n] : (uint8_t)0;
+    double s[3] = {0, 0, 0};
+    for (int r = 0; r < nc; r++) {
+        const int ei = i - kCXd(r), ej = j - kCYd(r), ek = g.dim == 3 ? k - kCZd(r) : 0;
+        if (ei < 0 || ej < 0 || ei >= g.nel[0] || ej >= g.nel[1]) continue;
+        if (g.dim == 3 && (ek < 0 || ek >= g.nel[2])) continue;
+        const long long e = g.dim == 3 ? ((long long)ei * g.nel[1] + ej) * g.nel[2] + ek : (long long)ei * g.nel[1] + ej;
+        const double we = E[e];
+        for (int d = 0; d < dof; d++) s[d] += kd.d[r * dof + d] * we;
+    }
+    for (int d = 0; d < dof; d++) diag[n * dof + d] = (m & (1 << d)) ? T(1) : (T)s[d];
+}
+
+template <typename T>
+int launch_diagonal(const Op* op, const double* E, const uint8_t* mask, T* diag, cudaStream_t st) {
+    const Grid& g = op->grid;
+    KDiag kd;
+    const int nd = (g.dim == 3 ? 8 : 4) * g.dim;
+    for (int i = 0; i < nd; i++) kd.d[i] = op->K0[i * nd + i];
+    k_diagonal<T><<<(unsigned)((g.n_nodes + 255) / 256), 256, 0, st>>>(g, E, mask, kd, diag);
+    PF_LAUNCH_CHECK("diagonal launch");
+    return PF_OK;
+}
+template int launch_diagonal<double>(const Op*, const double*, const uint8_t*, double*, cudaStream_t);
+template int launch_diagonal<float>(const Op*, const double*, const uint8_t*, float*, cudaStream_t);
+
+// dk_e = -(T u_e)^T B (T u_e) (H8) ; dense quadratic form (Q4)
+__global__ void k_sens_h8(int NX, int NY, int NZ, const double* __restrict__ U, const H8Blk<double> blk,
+                          double* __restrict__ dk) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)NX * NY * NZ) return;
+    const int k = (int)(e % NZ), j = (int)((e / NZ) % NY), i = (int)(e / ((long long)NY * NZ));
+    const int nx = NX + 1, nz = NZ + 1;
+    double v[3][2][2][2];  // [comp][a][b][c] corner values -> Walsh coefficients in place
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const long long n = (long long)(k + c) + (long long)nz * ((i + a) + (long long)nx * (j + b));
+#pragma unroll
+                for (int d = 0; d < 3; d++) v[d][a][b][c] = U[3 * n + d];
+            }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const double x0 = v[d][0][b][c], x1 = v[d][1][b][c];
+                v[d][0][b][c] = x0 + x1;
+                v[d][1][b][c] = x1 - x0;
+            }
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const double x0 = v[d][a][0][c], x1 = v[d][a][1][c];
+                v[d][a][0][c] = x0 + x1;
+                v[d][a][1][c] = x1 - x0;
+            }
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const double x0 = v[d][a][b][0], x1 = v[d][a][b][1];
+                v[d][a][b][0] = x0 + x1;
+                v[d][a][b][1] = x1 - x0;
+            }
+    }
+    double q = 0.0;
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        const int px = p & 1, py = (p >> 1) & 1, pz = (p >> 2) & 1;
+        const double i0 = v[0][px ^ 1][py][pz], i1 = v[1][px][py ^ 1][pz], i2 = v[2][px][py][pz ^ 1];
+        const double o0 = blk.b[p][0][0] * i0 + blk.b[p][0][1] * i1 + blk.b[p][0][2] * i2;
+        const double o1 = blk.b[p][1][0] * i0 + blk.b[p][1][1] * i1 + blk.b[p][1][2] * i2;
+        const double o2 = blk.b[p][2][0] * i0 + blk.b[p][2][1] * i1 + blk.b[p][2][2] * i2;
+        q += i0 * o0 + i1 * o1 + i2 * o2;
+    }
+    dk[e] = -q;
+}
+
+__global__ void k_sens_q4(int NX, int NY, const double* __restrict__ U, const Q4K<double> K, double* __restrict__ dk) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)NX * NY) return;
+    const int i = (int)(e / NY), j = (int)(e % NY), nx = NX + 1;
+    double ue[8];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const long long m = (long long)(i + kCXd(q)) + (long long)nx * (j + kCYd(q));
+        ue[2 * q] = U[2 * m];
+        ue[2 * q + 1] = U[2 * m + 1];
+    }
+    double out = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) s += K.k[a][b] * ue[b];
+        out -= s * ue[a];
+    }
+    dk[e] = out;
+}
+
+int launch_sensitivity(const Op* op, const double* U, double* dk, cudaStream_t st) {
+    const Grid& g = op->grid;
+    const unsigned nb = (unsigned)((g.n_elem + 255) / 256);
+    if (g.dim == 3)
+        k_sens_h8<<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], U, make_blk<double>(op), dk);
+    else
+        k_sens_q4<<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], U, make_q4k<double>(op), dk);
+    PF_LAUNCH_CHECK("sensitivity launch");
+    return PF_OK;
+}
+
+__global__ void k_pack_mask(long long n_nodes, int dof, const uint8_t* __restrict__ con, uint8_t* __restrict__ mask) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= n_nodes) return;
+    uint8_t m = 0;
+    for (int d = 0; d < dof; d++)
+        if (con[n * dof + d]) m |= (uint8_t)(1 << d);
+    mask[n] = m;
+}
+
+int launch_pack_mask(const Op* op, const uint8_t* con, uint8_t* mask, cudaStream_t st) {
+    const Grid& g = op->grid;
+    k_pack_mask<<<(unsigned)((g.n_nodes + 255) / 256), 256, 0, st>>>(g.n_nodes, g.dof, con, mask);
+    PF_LAUNCH_CHECK("pack mask launch");
+    return PF_OK;
+}
+
+}  // namespace pf

@@ -1,0 +1,578 @@
+// Multigrid level kernels: grid transfers, Galerkin coarse operators, block-stencil
+// matvec with the shared epilogues, stencil diagonal and dense export of the coarsest
+// operator.  All kernels are generic over the dimension (DIM = 2 or 3, dof = DIM).
+//
+// Transfer operators follow the reference (pyFANTOM/core/CUDA/Kernels/mgm.cu:1-244):
+// restriction R = diag(1/tw) Phat^T and prolongation P = Phat diag(1/tw) = R^T, where Phat
+// is trilinear (bilinear) interpolation (weights 0.5^{|d|_1} on the 3^DIM fine nodes
+// around an even fine node) and tw(c) = prod over axes of (1.5 on a boundary, else 2).
+// Coarse operators are Galerkin R A P with A_fine = Z K Z + I - Z on level 0
+// (mgm.cu:247-447) and R A_l P on deeper levels (mgm.cu:449-590).
+#include "common.cuh"
+#include "elemop.cuh"
+#include "mgkern.cuh"
+
+namespace pf {
+
+template <int DIM>
+struct GridDev {
+    int nel[3];
+    int nn[3];
+    long long n_nodes;
+};
+
+template <int DIM>
+__host__ __device__ __forceinline__ long long nidx(const GridDev<DIM>& g, int i, int j, int k) {
+    if (DIM == 3) return (long long)k + (long long)g.nn[2] * (i + (long long)g.nn[0] * j);
+    return (long long)i + (long long)g.nn[0] * j;
+}
+template <int DIM>
+__device__ __forceinline__ void ndec(const GridDev<DIM>& g, long long n, int& i, int& j, int& k) {
+    if (DIM == 3) {
+        k = (int)(n % g.nn[2]);
+        const long long t = n / g.nn[2];
+        i = (int)(t % g.nn[0]);
+        j = (int)(t / g.nn[0]);
+    } else {
+        i = (int)(n % g.nn[0]);
+        j = (int)(n / g.nn[0]);
+        k = 0;
+    }
+}
+template <int DIM>
+__device__ __forceinline__ bool nok(const GridDev<DIM>& g, int i, int j, int k) {
+    if (i < 0 || j < 0 || i >= g.nn[0] || j >= g.nn[1]) return false;
+    if (DIM == 3 && (k < 0 || k >= g.nn[2])) return false;
+    return true;
+}
+template <int DIM>
+__device__ __forceinline__ double total_weight(const GridDev<DIM>& gc, int i, int j, int k) {
+    double t = ((i == 0 || i == gc.nn[0] - 1) ? 1.5 : 2.0) * ((j == 0 || j == gc.nn[1] - 1) ? 1.5 : 2.0);
+    if (DIM == 3) t *= (k == 0 || k == gc.nn[2] - 1) ? 1.5 : 2.0;
+    return t;
+}
+__device__ __forceinline__ double half_pow(int d) { return d == 0 ? 1.0 : d == 1 ? 0.5 : d == 2 ? 0.25 : 0.125; }
+
+template <int DIM>
+static GridDev<DIM> gdev(const Grid& g) {
+    GridDev<DIM> d;
+    for (int a = 0; a < 3; a++) {
+        d.nel[a] = g.nel[a];
+        d.nn[a] = g.nn[a];
+    }
+    d.n_nodes = g.n_nodes;
+    return d;
+}
+
+// ---------------------------------------------------------------------------------------
+// transfers
+// ---------------------------------------------------------------------------------------
+template <int DIM, typename TI, typename TO>
+__global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restrict__ vf, TO* __restrict__ vc,
+                           const int* skip) {
+    if (skip && *skip) return;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= gc.n_nodes) return;
+    int ic, jc, kc;
+    ndec(gc, c, ic, jc, kc);
+    const double inv_tw = 1.0 / total_weight(gc, ic, jc, kc);
+    double acc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) acc[d] = 0.0;
+    constexpr int KR = DIM == 3 ? 1 : 0;
+#pragma unroll
+    for (int di = -1; di <= 1; di++)
+#pragma unroll
+        for (int dj = -1; dj <= 1; dj++)
+#pragma unroll
+            for (int dk = -KR; dk <= KR; dk++) {
+                const int fi = 2 * ic + di, fj = 2 * jc + dj, fk = 2 * kc + dk;
+                if (!nok(gf, fi, fj, fk)) continue;
+                const double w = half_pow((di != 0) + (dj != 0) + (dk != 0));
+                const long long n = nidx(gf, fi, fj, fk);
+#pragma unroll
+                for (int d = 0; d < DIM; d++) acc[d] += w * (double)vf[n * DIM + d];
+            }
+#pragma unroll
+    for (int d = 0; d < DIM; d++) vc[c * DIM + d] = (TO)(acc[d] * inv_tw);
+}
+
+template <int DIM, typename T>
+__global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict__ vc, T* __restrict__ vf,
+                          const int* skip) {
+    if (skip && *skip) return;
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= gf.n_nodes) return;
+    int i, j, k;
+    ndec(gf, f, i, j, k);
+    double acc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) acc[d] = 0.0;
+    int count = 0;
+    const int k0 = DIM == 3 ? k / 2 : 0, k1 = DIM == 3 ? k / 2 + (k & 1) : 0;
+    for (int ci = i / 2; ci <= i / 2 + (i & 1); ci++) {
+        if (ci >= gc.nn[0]) continue;
+        for (int cj = j / 2; cj <= j / 2 + (j & 1); cj++) {
+            if (cj >= gc.nn[1]) continue;
+            for (int ck = k0; ck <= k1; ck++) {
+                if (DIM == 3 && ck >= gc.nn[2]) continue;
+                const double itw = 1.0 / total_weight(gc, ci, cj, ck);
+                const long long n = nidx(gc, ci, cj, ck);
+#pragma unroll
+                for (int d = 0; d < DIM; d++) acc[d] += (double)vc[n * DIM + d] * itw;
+                count++;
+            }
+        }
+    }
+    const double ic = count > 0 ? 1.0 / count : 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) vf[f * DIM + d] = (T)(acc[d] * ic);
+}
+
+template <typename TI, typename TO>
+int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st) {
+    const Grid gc = coarse_grid(gf);
+    const unsigned nb = (unsigned)((gc.n_nodes + 255) / 256);
+    if (gf.dim == 3)
+        k_restrict<3, TI, TO><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vf, vc, skip);
+    else
+        k_restrict<2, TI, TO><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), vf, vc, skip);
+    PF_LAUNCH_CHECK("restrict launch");
+    return PF_OK;
+}
+template <typename T>
+int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st) {
+    const Grid gc = coarse_grid(gf);
+    const unsigned nb = (unsigned)((gf.n_nodes + 255) / 256);
+    if (gf.dim == 3)
+        k_prolong<3, T><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vc, vf, skip);
+    else
+        k_prolong<2, T><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), vc, vf, skip);
+    PF_LAUNCH_CHECK("prolong launch");
+    return PF_OK;
+}
+template int launch_restrict<double, double>(const Grid&, const double*, double*, const int*, cudaStream_t);
+template int launch_restrict<float, float>(const Grid&, const float*, float*, const int*, cudaStream_t);
+template int launch_prolong<double>(const Grid&, const double*, double*, const int*, cudaStream_t);
+template int launch_prolong<float>(const Grid&, const float*, float*, const int*, cudaStream_t);
+
+// ---------------------------------------------------------------------------------------
+// block-stencil matvec (levels >= 1): y_n = sum_o A[n,o] u_{n+o}
+// ---------------------------------------------------------------------------------------
+template <int DIM, typename T>
+__global__ void __launch_bounds__(256) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
+                                                         const T* __restrict__ u, Epi<T> epi) {
+    __shared__ double s_red[8];
+    if (epi.skip && *epi.skip) return;
+    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dot = 0.0;
+    const T wgt = epi_omega(epi);
+    if (n < g.n_nodes) {
+        int i, j, k;
+        ndec(g, n, i, j, k);
+        T acc[DIM];
+#pragma unroll
+        for (int a = 0; a < DIM; a++) acc[a] = T(0);
+        const long long N = g.n_nodes;
+#pragma unroll
+        for (int o = 0; o < NB; o++) {
+            const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = DIM == 3 ? o / 9 - 1 : 0;
+            if (!nok(g, i + ox, j + oy, k + oz)) continue;
+            const long long m = nidx(g, i + ox, j + oy, k + oz);
+            T um[DIM];
+#pragma unroll
+            for (int b = 0; b < DIM; b++) um[b] = u[m * DIM + b];
+#pragma unroll
+            for (int a = 0; a < DIM; a++)
+#pragma unroll
+                for (int b = 0; b < DIM; b++) acc[a] = fma(A[((long long)(o * BS + a * DIM + b)) * N + n], um[b], acc[a]);
+        }
+#pragma unroll
+        for (int a = 0; a < DIM; a++) {
+            const long long gi = n * DIM + a;
+            const T o = epi_apply(epi, gi, acc[a], wgt);
+            epi.out[gi] = o;
+            if (epi.dot_partial) dot += (double)epi.dot_a[gi] * (double)(epi.dot_of_y ? acc[a] : o);
+        }
+    }
+    if (epi.dot_partial) {
+        const double s = block_sum<256>(dot, s_red);
+        if (threadIdx.x == 0) epi.dot_partial[blockIdx.x] = s;
+    }
+}
+
+template <typename T>
+int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st) {
+    const unsigned nb = (unsigned)((g.n_nodes + 255) / 256);
+    if (g.dim == 3)
+        k_stencil_matvec<3, T><<<nb, 256, 0, st>>>(gdev<3>(g), A, u, epi);
+    else
+        k_stencil_matvec<2, T><<<nb, 256, 0, st>>>(gdev<2>(g), A, u, epi);
+    PF_LAUNCH_CHECK("stencil matvec launch");
+    return PF_OK;
+}
+long long stencil_matvec_num_blocks(const Grid& g) { return (g.n_nodes + 255) / 256; }
+template int launch_stencil_matvec<double>(const Grid&, const double*, const double*, const Epi<double>&,
+                                           cudaStream_t);
+template int launch_stencil_matvec<float>(const Grid&, const float*, const float*, const Epi<float>&, cudaStream_t);
+
+// ---------------------------------------------------------------------------------------
+// Galerkin level 1 from the element operator.
+// With Phat_c the local interpolation from a coarse element's corners to its child c,
+//   Phat^T (Z K Z) Phat = sum_C sum_c E_{C,c} (Z Phat_c)^T K0 (Z Phat_c)
+// which for a coarse element C whose 3^DIM fine nodes carry no constraint is
+// sum_c E_{C,c} Kc[c] with the fixed child matrices Kc[c] = Phat_c^T K0 Phat_c.  The
+// identity rows of constrained DOFs add Phat^T (I - Z) Phat.  Each thread produces one
+// dof x dof block (coarse node I, neighbour o) by gathering the coarse elements that
+// contain I and I+o (owner computes, no atomics), then scales by 1/(tw_I tw_J).
+// ---------------------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ int ccx(int l) {
+    return kCXd(l);
+}
+
+// flags: per coarse element, 1 if any of its fine nodes has a constraint;
+//        per coarse node, 1 if any fine node within distance 1 of 2I has a constraint.
+template <int DIM>
+__global__ void k_coarse_flags(GridDev<DIM> gf, GridDev<DIM> gc, const uint8_t* __restrict__ mask,
+                               uint8_t* __restrict__ elem_flag, uint8_t* __restrict__ node_flag) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= gc.n_nodes) return;
+    int ic, jc, kc;
+    ndec(gc, c, ic, jc, kc);
+    constexpr int KR = DIM == 3 ? 1 : 0;
+    uint8_t nf = 0;
+    for (int di = -1; di <= 1; di++)
+        for (int dj = -1; dj <= 1; dj++)
+            for (int dk = -KR; dk <= KR; dk++) {
+                const int fi = 2 * ic + di, fj = 2 * jc + dj, fk = 2 * kc + dk;
+                if (nok(gf, fi, fj, fk) && mask[nidx(gf, fi, fj, fk)]) nf = 1;
+            }
+    node_flag[c] = nf;
+    // coarse element with lower corner (ic, jc, kc)
+    const bool has_elem = ic < gc.nel[0] && jc < gc.nel[1] && (DIM == 2 || kc < gc.nel[2]);
+    if (has_elem) {
+        uint8_t ef = 0;
+        for (int di = 0; di <= 2; di++)
+            for (int dj = 0; dj <= 2; dj++)
+                for (int dk = 0; dk <= 2 * KR; dk++)
+                    if (mask[nidx(gf, 2 * ic + di, 2 * jc + dj, 2 * kc + dk)]) ef = 1;
+        const long long e = DIM == 3 ? ((long long)ic * gc.nel[1] + jc) * gc.nel[2] + kc : (long long)ic * gc.nel[1] + jc;
+        elem_flag[e] = ef;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_galerkin_l0(GridDev<DIM> gf, GridDev<DIM> gc, const double* __restrict__ E,
+                                                      const uint8_t* __restrict__ mask,
+                                                      const uint8_t* __restrict__ elem_flag,
+                                                      const uint8_t* __restrict__ node_flag,
+                                                      const double* __restrict__ K0,  // (NC*DIM)^2
+                                                      const double* __restrict__ Kc,  // NC x (NC*DIM)^2
+                                                      double* __restrict__ A) {
+    constexpr int NC = DIM == 3 ? 8 : 4, ND = NC * DIM, NB = DIM == 3 ? 27 : 9, BS = DIM * DIM;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long Nc = gc.n_nodes;
+    if (tid >= Nc * NB) return;
+    const int o = (int)(tid / Nc);
+    const long long I = tid - (long long)o * Nc;
+    int ic, jc, kc;
+    ndec(gc, I, ic, jc, kc);
+    const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = DIM == 3 ? o / 9 - 1 : 0;
+    double blk[BS];
+#pragma unroll
+    for (int a = 0; a < BS; a++) blk[a] = 0.0;
+    const int ti = ic + ox, tj = jc + oy, tk = kc + oz;
+    if (nok(gc, ti, tj, tk)) {
+        // coarse elements containing I as local corner LI
+        for (int LI = 0; LI < NC; LI++) {
+            const int ex = ic - kCXd(LI), ey = jc - kCYd(LI), ez = DIM == 3 ? kc - kCZd(LI) : 0;
+            if (ex < 0 || ey < 0 || ex >= gc.nel[0] || ey >= gc.nel[1]) continue;
+            if (DIM == 3 && (ez < 0 || ez >= gc.nel[2])) continue;
+            // J must be a corner of the same element
+            const int lx = kCXd(LI) + ox, ly = kCYd(LI) + oy, lz = DIM == 3 ? kCZd(LI) + oz : 0;
+            if (lx < 0 || lx > 1 || ly < 0 || ly > 1 || lz < 0 || lz > 1) continue;
+            int LJ = 0;
+            for (int q = 0; q < NC; q++)
+                if (kCXd(q) == lx && kCYd(q) == ly && (DIM == 2 || kCZd(q) == lz)) LJ = q;
+            const long long ce = DIM == 3 ? ((long long)ex * gc.nel[1] + ey) * gc.nel[2] + ez : (long long)ex * gc.nel[1] + ey;
+            const bool dirty = elem_flag[ce] != 0;
+            for (int c = 0; c < NC; c++) {
+                const int fx = 2 * ex + kCXd(c), fy = 2 * ey + kCYd(c), fz = DIM == 3 ? 2 * ez + kCZd(c) : 0;
+                const long long fe = DIM == 3 ? ((long long)fx * gf.nel[1] + fy) * gf.nel[2] + fz : (long long)fx * gf.nel[1] + fy;
+                const double we = E[fe];
+                if (!dirty) {
+                    const double* kc_ = Kc + (long long)c * ND * ND;
+#pragma unroll
+                    for (int a = 0; a < DIM; a++)
+#pragma unroll
+                        for (int b = 0; b < DIM; b++) blk[a * DIM + b] += we * __ldg(kc_ + (LI * DIM + a) * ND + LJ * DIM + b);
+                } else {
+                    // masked child: sum_{l,l2} Phat_c[l][LI] z(l,a) K0[(l,a),(l2,b)] z(l2,b) Phat_c[l2][LJ]
+                    for (int l = 0; l < NC; l++) {
+                        const int nxl = kCXd(c) + kCXd(l), nyl = kCYd(c) + kCYd(l), nzl = DIM == 3 ? kCZd(c) + kCZd(l) : 0;
+                        double pl = (1.0 - 0.5 * abs(nxl - 2 * kCXd(LI))) * (1.0 - 0.5 * abs(nyl - 2 * kCYd(LI)));
+                        if (DIM == 3) pl *= 1.0 - 0.5 * abs(nzl - 2 * kCZd(LI));
+                        if (pl == 0.0) continue;
+                        const uint8_t ml = mask[nidx(gf, 2 * ex + nxl, 2 * ey + nyl, 2 * ez + nzl)];
+                        for (int l2 = 0; l2 < NC; l2++) {
+                            const int nx2 = kCXd(c) + kCXd(l2), ny2 = kCYd(c) + kCYd(l2), nz2 = DIM == 3 ? kCZd(c) + kCZd(l2) : 0;
+                            double p2 = (1.0 - 0.5 * abs(nx2 - 2 * kCXd(LJ))) * (1.0 - 0.5 * abs(ny2 - 2 * kCYd(LJ)));
+                            if (DIM == 3) p2 *= 1.0 - 0.5 * abs(nz2 - 2 * kCZd(LJ));
+                            if (p2 == 0.0) continue;
+                            const uint8_t m2 = mask[nidx(gf, 2 * ex + nx2, 2 * ey + ny2, 2 * ez + nz2)];
+                            const double f = we * pl * p2;
+                            for (int a = 0; a < DIM; a++) {
+                                if (ml & (1 << a)) continue;
+                                for (int b = 0; b < DIM; b++) {
+                                    if (m2 & (1 << b)) continue;
+                                    blk[a * DIM + b] += f * K0[(l * DIM + a) * ND + l2 * DIM + b];
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        // identity rows of constrained fine DOFs: sum_n Phat[n,I] Phat[n,J] on the diagonal
+        if (node_flag[I]) {
+            constexpr int KR = DIM == 3 ? 1 : 0;
+            for (int di = -1; di <= 1; di++)
+                for (int dj = -1; dj <= 1; dj++)
+                    for (int dk = -KR; dk <= KR; dk++) {
+                        const int fi = 2 * ic + di, fj = 2 * jc + dj, fk = 2 * kc + dk;
+                        if (!nok(gf, fi, fj, fk)) continue;
+                        const int ei = fi - 2 * ti, ej = fj - 2 * tj, ek = fk - 2 * tk;
+                        if (ei < -1 || ei > 1 || ej < -1 || ej > 1 || ek < -1 || ek > 1) continue;
+                        const uint8_t m = mask[nidx(gf, fi, fj, fk)];
+                        if (!m) continue;
+                        const double w = half_pow((di != 0) + (dj != 0) + (dk != 0)) *
+                                         half_pow((ei != 0) + (ej != 0) + (ek != 0));
+                        for (int a = 0; a < DIM; a++)
+                            if (m & (1 << a)) blk[a * DIM + a] += w;
+                    }
+        }
+        const double s = 1.0 / (total_weight(gc, ic, jc, kc) * total_weight(gc, ti, tj, tk));
+#pragma unroll
+        for (int a = 0; a < BS; a++) blk[a] *= s;
+    }
+#pragma unroll
+    for (int a = 0; a < BS; a++) A[((long long)(o * BS + a)) * Nc + I] = blk[a];
+}
+
+// child matrices Kc[c] = Phat_c^T K0 Phat_c (host)
+void galerkin_child_matrices(int dim, const double* K0, double* Kc) {
+    const int NC = dim == 3 ? 8 : 4, ND = NC * dim;
+    for (int c = 0; c < NC; c++) {
+        double P[8][8];  // P[l][L]: weight of coarse corner L at child corner l
+        for (int l = 0; l < NC; l++)
+            for (int L = 0; L < NC; L++) {
+                const int fx = kCXd(c) + kCXd(l), fy = kCYd(c) + kCYd(l), fz = dim == 3 ? kCZd(c) + kCZd(l) : 0;
+                double w = (1.0 - 0.5 * abs(fx - 2 * kCXd(L))) * (1.0 - 0.5 * abs(fy - 2 * kCYd(L)));
+                if (dim == 3) w *= 1.0 - 0.5 * abs(fz - 2 * kCZd(L));
+                P[l][L] = w;
+            }
+        double* out = Kc + (long long)c * ND * ND;
+        for (int L = 0; L < NC; L++)
+            for (int a = 0; a < dim; a++)
+                for (int L2 = 0; L2 < NC; L2++)
+                    for (int b = 0; b < dim; b++) {
+                        double s = 0.0;
+                        for (int l = 0; l < NC; l++) {
+                            if (P[l][L] == 0.0) continue;
+                            for (int l2 = 0; l2 < NC; l2++) {
+                                if (P[l2][L2] == 0.0) continue;
+                                s += P[l][L] * K0[(l * dim + a) * ND + l2 * dim + b] * P[l2][L2];
+                            }
+                        }
+                        out[(L * dim + a) * ND + L2 * dim + b] = s;
+                    }
+    }
+}
+
+int launch_coarse_flags(const Grid& gf, const uint8_t* mask, uint8_t* elem_flag, uint8_t* node_flag, cudaStream_t st) {
+    const Grid gc = coarse_grid(gf);
+    const unsigned nb = (unsigned)((gc.n_nodes + 255) / 256);
+    if (gf.dim == 3)
+        k_coarse_flags<3><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), mask, elem_flag, node_flag);
+    else
+        k_coarse_flags<2><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), mask, elem_flag, node_flag);
+    PF_LAUNCH_CHECK("coarse flags launch");
+    return PF_OK;
+}
+
+int launch_galerkin_l0(const Grid& gf, const double* E, const uint8_t* mask, const uint8_t* elem_flag,
+                       const uint8_t* node_flag, const double* K0_dev, const double* Kc_dev, double* A, cudaStream_t st) {
+    const Grid gc = coarse_grid(gf);
+    const int NB = gf.dim == 3 ? 27 : 9;
+    const long long n = gc.n_nodes * NB;
+    const unsigned nb = (unsigned)((n + 127) / 128);
+    if (gf.dim == 3)
+        k_galerkin_l0<3><<<nb, 128, 0, st>>>(gdev<3>(gf), gdev<3>(gc), E, mask, elem_flag, node_flag, K0_dev, Kc_dev, A);
+    else
+        k_galerkin_l0<2><<<nb, 128, 0, st>>>(gdev<2>(gf), gdev<2>(gc), E, mask, elem_flag, node_flag, K0_dev, Kc_dev, A);
+    PF_LAUNCH_CHECK("galerkin l0 launch");
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Galerkin level l+1 from the level-l block stencil:
+//   A_c[I,J] = sum_{n in supp I} sum_{m in supp J, |m-n|<=1} Phat[n,I] A[n, m-n] Phat[m,J] / (tw_I tw_J)
+// Per axis, the admissible (dn, dm) offset pairs depend only on the neighbour offset o.
+// ---------------------------------------------------------------------------------------
+__constant__ int c_pairs[3][7][2];  // [o+1][pair][dn, dm]
+__constant__ int c_npairs[3];
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_galerkin_l1p(GridDev<DIM> gf, GridDev<DIM> gc, const double* __restrict__ Af,
+                                                       double* __restrict__ Ac) {
+    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long Nc = gc.n_nodes, Nf = gf.n_nodes;
+    if (tid >= Nc * NB) return;
+    const int o = (int)(tid / Nc);
+    const long long I = tid - (long long)o * Nc;
+    int ic, jc, kc;
+    ndec(gc, I, ic, jc, kc);
+    const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = DIM == 3 ? o / 9 - 1 : 0;
+    double blk[BS];
+#pragma unroll
+    for (int a = 0; a < BS; a++) blk[a] = 0.0;
+    const int ti = ic + ox, tj = jc + oy, tk = kc + oz;
+    if (nok(gc, ti, tj, tk)) {
+        const int npx = c_npairs[ox + 1], npy = c_npairs[oy + 1], npz = DIM == 3 ? c_npairs[oz + 1] : 1;
+        for (int px = 0; px < npx; px++) {
+            const int dnx = c_pairs[ox + 1][px][0], dmx = c_pairs[ox + 1][px][1];
+            const int nx_ = 2 * ic + dnx, mx = 2 * ti + dmx;
+            if (nx_ < 0 || nx_ >= gf.nn[0] || mx < 0 || mx >= gf.nn[0]) continue;
+            for (int py = 0; py < npy; py++) {
+                const int dny = c_pairs[oy + 1][py][0], dmy = c_pairs[oy + 1][py][1];
+                const int ny_ = 2 * jc + dny, my = 2 * tj + dmy;
+                if (ny_ < 0 || ny_ >= gf.nn[1] || my < 0 || my >= gf.nn[1]) continue;
+                for (int pz = 0; pz < npz; pz++) {
+                    int dnz = 0, dmz = 0, nz_ = 0, mz = 0;
+                    if (DIM == 3) {
+                        dnz = c_pairs[oz + 1][pz][0];
+                        dmz = c_pairs[oz + 1][pz][1];
+                        nz_ = 2 * kc + dnz;
+                        mz = 2 * tk + dmz;
+                        if (nz_ < 0 || nz_ >= gf.nn[2] || mz < 0 || mz >= gf.nn[2]) continue;
+                    }
+                    const double w = half_pow((dnx != 0) + (dny != 0) + (dnz != 0)) *
+                                     half_pow((dmx != 0) + (dmy != 0) + (dmz != 0));
+                    const long long n = nidx(gf, nx_, ny_, nz_);
+                    const int rx = mx - nx_, ry = my - ny_, rz = DIM == 3 ? mz - nz_ : 0;
+                    const int on = (rx + 1) + 3 * (ry + 1) + (DIM == 3 ? 9 * (rz + 1) : 0);
+#pragma unroll
+                    for (int a = 0; a < BS; a++) blk[a] += w * Af[((long long)(on * BS + a)) * Nf + n];
+                }
+            }
+        }
+        const double s = 1.0 / (total_weight(gc, ic, jc, kc) * total_weight(gc, ti, tj, tk));
+#pragma unroll
+        for (int a = 0; a < BS; a++) blk[a] *= s;
+    }
+#pragma unroll
+    for (int a = 0; a < BS; a++) Ac[((long long)(o * BS + a)) * Nc + I] = blk[a];
+}
+
+static bool g_pairs_ready = false;
+static int init_pairs() {
+    if (g_pairs_ready) return PF_OK;
+    int pairs[3][7][2] = {};
+    int np[3] = {0, 0, 0};
+    for (int o = -1; o <= 1; o++)
+        for (int dn = -1; dn <= 1; dn++)
+            for (int dm = -1; dm <= 1; dm++) {
+                const int r = 2 * o + dm - dn;
+                if (r < -1 || r > 1) continue;
+                pairs[o + 1][np[o + 1]][0] = dn;
+                pairs[o + 1][np[o + 1]][1] = dm;
+                np[o + 1]++;
+            }
+    PF_CUDA(cudaMemcpyToSymbol(c_pairs, pairs, sizeof(pairs)));
+    PF_CUDA(cudaMemcpyToSymbol(c_npairs, np, sizeof(np)));
+    g_pairs_ready = true;
+    return PF_OK;
+}
+
+int launch_galerkin_l1p(const Grid& gf, const double* Af, double* Ac, cudaStream_t st) {
+    int s = init_pairs();
+    if (s) return s;
+    const Grid gc = coarse_grid(gf);
+    const int NB = gf.dim == 3 ? 27 : 9;
+    const unsigned nb = (unsigned)((gc.n_nodes * NB + 127) / 128);
+    if (gf.dim == 3)
+        k_galerkin_l1p<3><<<nb, 128, 0, st>>>(gdev<3>(gf), gdev<3>(gc), Af, Ac);
+    else
+        k_galerkin_l1p<2><<<nb, 128, 0, st>>>(gdev<2>(gf), gdev<2>(gc), Af, Ac);
+    PF_LAUNCH_CHECK("galerkin l1p launch");
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// stencil diagonal -> inverse diagonal, precision conversion, dense export
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_stencil_dinv(long long N, int dim, const double* __restrict__ A, T* __restrict__ dinv) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * dim) return;
+    const long long n = t / dim;
+    const int a = (int)(t - n * dim);
+    const int oc = dim == 3 ? 13 : 4, BS = dim * dim;
+    dinv[t] = (T)(1.0 / A[((long long)(oc * BS + a * dim + a)) * N + n]);
+}
+
+template <typename T>
+int launch_stencil_dinv(const Grid& g, const double* A, T* dinv, cudaStream_t st) {
+    const long long n = g.n_nodes * g.dim;
+    k_stencil_dinv<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g.n_nodes, g.dim, A, dinv);
+    PF_LAUNCH_CHECK("stencil dinv launch");
+    return PF_OK;
+}
+template int launch_stencil_dinv<double>(const Grid&, const double*, double*, cudaStream_t);
+template int launch_stencil_dinv<float>(const Grid&, const double*, float*, cudaStream_t);
+
+template <int DIM>
+__global__ void k_stencil_to_dense(GridDev<DIM> g, const double* __restrict__ A, double* __restrict__ M, long long ld) {
+    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long N = g.n_nodes;
+    if (t >= N * NB * BS) return;
+    const long long n = t % N;
+    const int ob = (int)(t / N);
+    const int o = ob / BS, ab = ob % BS, a = ab / DIM, b = ab % DIM;
+    int i, j, k;
+    ndec(g, n, i, j, k);
+    const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = DIM == 3 ? o / 9 - 1 : 0;
+    if (!nok(g, i + ox, j + oy, k + oz)) return;
+    const long long m = nidx(g, i + ox, j + oy, k + oz);
+    M[(n * DIM + a) * ld + m * DIM + b] = A[t];
+}
+
+int launch_stencil_to_dense(const Grid& g, const double* A, double* M, long long ld, cudaStream_t st) {
+    const int NB = g.dim == 3 ? 27 : 9;
+    const long long n = g.n_nodes * NB * g.dim * g.dim;
+    if (g.dim == 3)
+        k_stencil_to_dense<3><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gdev<3>(g), A, M, ld);
+    else
+        k_stencil_to_dense<2><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gdev<2>(g), A, M, ld);
+    PF_LAUNCH_CHECK("stencil to dense launch");
+    return PF_OK;
+}
+
+__global__ void k_d2f(long long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+int launch_d2f(long long n, const double* a, float* b, cudaStream_t st) {
+    long long nb = (n + 255) / 256;
+    if (nb > 4 * kNumSM * 8) nb = 4 * kNumSM * 8;
+    if (nb < 1) nb = 1;
+    k_d2f<<<(unsigned)nb, 256, 0, st>>>(n, a, b);
+    PF_LAUNCH_CHECK("d2f launch");
+    return PF_OK;
+}
+
+}  // namespace pf

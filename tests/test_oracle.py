@@ -1,0 +1,164 @@
+"""CPU: the oracle and the host-side restatements against the reference's golden vectors.
+
+The golden fixtures were produced by running the reference pyFANTOM CPU code
+(tests/golden/make_golden.py); these tests pin the oracle before it is trusted as the
+checker of the CUDA path.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel, unit_K0
+from oracle import oracle as O
+from pyfantom_b200 import workloads
+from pyfantom_b200.geom import _unit_element, cone_weights
+from pyfantom_b200.physics import LinearElasticity
+
+
+@pytest.mark.parametrize("tag", ["h8_nu03", "h8_nu13", "h8_aniso", "q4_nu03", "q4_aniso"])
+def test_k0_matches_reference(golden, tag):
+    g = golden("k0")
+    K = LinearElasticity(E=1.0, nu=float(g[tag + "_nu"])).K(_unit_element(g[tag + "_h"]))
+    assert rel(K, g[tag]) < 1e-14
+
+
+def test_k0_properties():
+    for dim in (2, 3):
+        K = unit_K0(dim)
+        assert np.allclose(K, K.T, atol=1e-15)
+        w = np.linalg.eigvalsh(K)
+        assert w.min() > -1e-12
+        n_rigid = 3 if dim == 2 else 6
+        assert np.sum(np.abs(w) < 1e-10) == n_rigid
+        # rigid translations are in the null space (row sums per component vanish)
+        for d in range(dim):
+            t = np.zeros(K.shape[0])
+            t[d::dim] = 1.0
+            assert np.abs(K @ t).max() < 1e-14
+
+
+@pytest.mark.parametrize("tag", ["3d", "3d_odd", "2d", "2d_odd"])
+def test_operators(golden, tag):
+    g = golden("operators")
+    nel = tuple(int(v) for v in g[tag + "_nel"])
+    K0 = unit_K0(len(nel))
+    E, u, cons = g[tag + "_E"], g[tag + "_u"], g[tag + "_cons"]
+    assert rel(O.matvec(nel, K0, E, u), g[tag + "_y_free"]) < 1e-13
+    assert rel(O.matvec(nel, K0, E, u, cons), g[tag + "_y_con"]) < 1e-13
+    assert rel(O.diagonal(nel, K0, E), g[tag + "_diag_free"]) < 1e-13
+    assert rel(O.diagonal(nel, K0, E, cons), g[tag + "_diag_con"]) < 1e-13
+    assert rel(O.process_dk(nel, K0, u), g[tag + "_dk"]) < 1e-13
+
+
+def test_mesh_connectivity_matches_reference(golden):
+    g = golden("operators")
+    import torch
+    from pyfantom_b200 import geom
+    dev = torch.device("cpu")
+    for tag in ["3d", "3d_odd", "2d", "2d_odd"]:
+        nel = tuple(int(v) for v in g[tag + "_nel"])
+        orig = geom.device
+        geom.device = lambda: dev
+        try:
+            el = geom._structured_elements(np.array(nel)).numpy()
+            nodes = geom._structured_nodes(np.array(nel), np.array(nel, dtype=float)).numpy()
+        finally:
+            geom.device = orig
+        assert np.array_equal(el, g[tag + "_elements"])
+        assert np.array_equal(nodes, g[tag + "_nodes"])
+
+
+@pytest.mark.parametrize("tag", ["3d", "2d"])
+def test_transfers(golden, tag):
+    g = golden("transfers")
+    nel = tuple(int(v) for v in g[tag + "_nel"])
+    assert np.array_equal(O.restrict(nel, g[tag + "_vf"]), g[tag + "_restricted"])
+    assert np.array_equal(O.prolong(nel, g[tag + "_vc"]), g[tag + "_prolonged"])
+    # R = P^T
+    rng = np.random.default_rng(0)
+    vf = rng.standard_normal(O.n_nodes(nel) * len(nel))
+    vc = rng.standard_normal(O.n_nodes(O.coarse_nel(nel)) * len(nel))
+    assert abs(vc @ O.restrict(nel, vf) - vf @ O.prolong(nel, vc)) < 1e-12 * abs(vc @ O.restrict(nel, vf))
+
+
+@pytest.mark.parametrize("tag", ["3d", "2d"])
+def test_galerkin(golden, tag):
+    g = golden("transfers")
+    nel = tuple(int(v) for v in g["gal" + tag + "_nel"])
+    K0 = unit_K0(len(nel))
+    A1 = O.galerkin_l0(nel, K0, g["gal" + tag + "_E"], g["gal" + tag + "_cons"])
+    D1 = O.stencil_to_dense(O.coarse_nel(nel), A1)
+    assert rel(D1, g["gal" + tag + "_A1"]) < 1e-13
+    A2 = O.galerkin_l1p(O.coarse_nel(nel), A1)
+    D2 = O.stencil_to_dense(O.coarse_nel(O.coarse_nel(nel)), A2)
+    assert rel(D2, g["gal" + tag + "_A2"]) < 1e-13
+    assert np.allclose(D1, D1.T, atol=1e-14 * np.abs(D1).max())
+
+
+@pytest.mark.parametrize("tag", ["3d_r2", "3d_r25", "3d_aniso", "2d_r15", "2d_r3"])
+def test_filter(golden, tag):
+    g = golden("filters")
+    nel = tuple(int(v) for v in g[tag + "_nel"])
+    w, off = cone_weights(nel, g[tag + "_h"], float(g[tag + "_r"]))
+    assert np.array_equal(off, g[tag + "_offsets"])
+    assert rel(w, g[tag + "_weights"]) < 1e-15
+    nrm = O.filter_normalizer(nel, w, off)
+    assert rel(nrm, g[tag + "_normalizer"]) < 1e-14
+    assert rel(O.filter_fwd(nel, w, off, g[tag + "_v"]), g[tag + "_fwd"]) < 1e-14
+    assert rel(O.filter_adj(nel, w, off, nrm, g[tag + "_v"]), g[tag + "_adj"]) < 1e-14
+    # exact adjoint: <Hx, y> = <x, H^T y>
+    rng = np.random.default_rng(3)
+    x, y = rng.standard_normal(len(nrm)), rng.standard_normal(len(nrm))
+    lhs = O.filter_fwd(nel, w, off, x) @ y
+    assert abs(lhs - x @ O.filter_adj(nel, w, off, nrm, y)) < 1e-12 * max(1.0, abs(lhs))
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_oc_bitexact(golden, tag):
+    g = golden("oc")
+    x = g[tag + "_x"]
+    xn, steps = O.oc_update(x, g[tag + "_df"], 1.0 / x.size, float(g[tag + "_vf"]), float(g[tag + "_move"]))
+    assert np.array_equal(xn, g[tag + "_xnew"])
+    assert 20 <= steps <= 100
+
+
+@pytest.mark.parametrize("tag", ["plain", "heavy", "emul"])
+def test_penalize(golden, tag):
+    g = golden("penalize")
+    kw = {"plain": dict(penalty=3.0, void=1e-9), "heavy": dict(penalty=3.0, void=1e-9, heavyside=True, beta=4.0, eta=0.4),
+          "emul": dict(penalty=2.5, void=1e-6, E_mul=2.0)}[tag]
+    assert rel(O.penalize(g["rho"], **kw), g[tag + "_E"]) < 1e-14
+    kg = {k: v for k, v in kw.items() if k != "void"}
+    assert rel(O.penalize_grad(g["rho"], **kg), g[tag + "_dE"]) < 1e-13
+
+
+def test_mgcg_oracle_matches_direct_solve(golden):
+    g = golden("solve16")
+    wl = workloads.cantilever3d(16, 8, 8, 0)
+    assert np.array_equal(wl["E"], g["E"]) and np.array_equal(wl["rhs"], g["rhs"])
+    K0 = unit_K0(3)
+    for nl in (1, 2, 3):
+        x, it, res, st = O.mgcg_solve(wl["nel"], K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=nl, tol=1e-10)
+        assert st == 0 and res < 1e-10
+        r = wl["rhs"] - O.matvec(wl["nel"], K0, wl["E"], x, wl["fixed_dofs"])
+        assert np.linalg.norm(r) / np.linalg.norm(wl["rhs"]) < 2e-10
+        assert rel(x, g["direct_U"]) < 1e-9
+        assert abs(wl["rhs"] @ x - float(g["direct_compliance"])) < 1e-9 * float(g["direct_compliance"])
+
+
+def test_known_answers_file():
+    ka = json.load(open(os.path.join(GOLDEN, "known_answers.json")))
+    assert ka["mbb_120x40"]["f_init"] == pytest.approx(1026.8430675962559, rel=1e-15)
+    assert ka["mbb_120x40"]["f_iter50"] == pytest.approx(202.13500765477625, rel=1e-15)
+
+
+def test_workloads():
+    wl = workloads.cantilever3d(8, 4, 4, 0)
+    assert wl["fixed_dofs"].size == 5 * 5 * 3
+    assert np.isclose(wl["rhs"].sum(), -1.0)
+    b = workloads.bridge3d(8, 4, 4, 0)
+    assert b["fixed_dofs"].size == 2 * 5 * 3
+    m = workloads.mbb2d(12, 4)
+    assert m["fixed_dofs"].size == 5 + 1

@@ -1,0 +1,208 @@
+"""GPU: V-cycle, MGCG, CG, failure statuses and the SIMP loop against the oracle and the
+reference goldens.
+
+Tolerances: the V-cycle is compared with the oracle's V-cycle to 1e-10 relative (same
+algorithm, different summation order); solves must reach the requested tolerance with
+a true FP64 residual below 2x the tolerance and agree with the oracle / reference direct
+solve to 1e-8 relative; compliance 1e-6 relative (the stated parity bar).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN, rel, unit_K0
+from oracle import oracle as O
+from pyfantom_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def setup_problem(wl, n_level, precision="fp64", tol=1e-10, maxiter=500, n_smooth=2, omega=0.6, solver="mg"):
+    from pyfantom_b200.CUDA import (CG, FiniteElement, MultiGrid, StructuredMesh2D, StructuredMesh3D,
+                                    StructuredStiffnessKernel)
+    from pyfantom_b200.physics import LinearElasticity
+    nel = wl["nel"]
+    phys = LinearElasticity(E=1.0, nu=0.3)
+    mesh = StructuredMesh3D(*nel, *nel, physics=phys) if len(nel) == 3 else StructuredMesh2D(*nel, *nel, physics=phys)
+    kern = StructuredStiffnessKernel(mesh)
+    if solver == "mg":
+        sol = MultiGrid(mesh, kern, maxiter=maxiter, tol=tol, n_smooth=n_smooth, omega=omega, n_level=n_level,
+                        precision=precision)
+    else:
+        sol = CG(kern, maxiter=maxiter, tol=tol)
+    fe = FiniteElement(mesh, kern, sol)
+    kern.add_constraints(torch.as_tensor(wl["fixed_dofs"], device="cuda"))
+    fe.rhs.copy_(torch.as_tensor(wl["rhs"], device="cuda"))
+    return mesh, kern, sol, fe
+
+
+def true_res(kern, U, rhs):
+    r = rhs - kern.dot(U)
+    return float(torch.linalg.norm(r) / torch.linalg.norm(rhs))
+
+
+@pytest.mark.parametrize("case", [("cant", (16, 8, 8), 2), ("cant", (32, 16, 16), 3), ("bridge", (16, 8, 8), 3),
+                                  ("mbb", (64, 32), 3)])
+def test_vcycle_matches_oracle(case):
+    kind, nel, nl = case
+    wl = (workloads.cantilever3d(*nel) if kind == "cant" else workloads.bridge3d(*nel) if kind == "bridge"
+          else workloads.mbb2d(*nel))
+    mesh, kern, sol, fe = setup_problem(wl, nl)
+    kern.set_rho(torch.as_tensor(wl["E"], device="cuda"))
+    sol.setup()
+    r = np.random.default_rng(0).standard_normal(kern.shape[0])
+    r[wl["fixed_dofs"]] = 0.0
+    z = sol.vcycle(torch.as_tensor(r, device="cuda"), omega=0.45).cpu().numpy()
+    zr = O.mg_vcycle(nel, unit_K0(len(nel)), wl["E"], wl["fixed_dofs"], r, n_level=nl, n_smooth=2, omega=0.45)
+    assert rel(z, zr) < 1e-10
+
+
+@pytest.mark.parametrize("case", [((16, 8, 8), 2), ((32, 16, 16), 3), ((24, 16, 8), 3)])
+def test_mgcg_matches_oracle(case):
+    nel, nl = case
+    wl = workloads.cantilever3d(*nel)
+    mesh, kern, sol, fe = setup_problem(wl, nl, tol=1e-10)
+    U, res = fe.solve(torch.as_tensor(wl["E"], device="cuda"))
+    xo, ito, reso, st = O.mgcg_solve(nel, unit_K0(3), wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=nl, tol=1e-10)
+    assert sol.last_info["status"] == "PF_OK" and res < 1e-10
+    assert abs(sol.last_info["iterations"] - ito) <= 1
+    assert true_res(kern, U, fe.rhs) < 2e-10
+    assert rel(U.cpu().numpy(), xo) < 1e-8
+
+
+def test_mgcg_matches_reference_solution(golden):
+    g = golden("solve16")
+    wl = workloads.cantilever3d(16, 8, 8)
+    mesh, kern, sol, fe = setup_problem(wl, 2, tol=1e-10)
+    U, res = fe.solve(torch.as_tensor(g["E"], device="cuda"))
+    c = float(torch.dot(fe.rhs, U))
+    assert abs(c - float(g["direct_compliance"])) < 1e-9 * abs(float(g["direct_compliance"]))
+    assert rel(U.cpu().numpy(), g["direct_U"]) < 1e-8
+    assert rel(U.cpu().numpy(), g["mg_U"]) < 1e-8
+
+
+@pytest.mark.parametrize("nel", [(32, 16, 16), (64, 32)])
+def test_mixed_precision_reaches_fp64_tolerance(nel):
+    wl = workloads.cantilever3d(*nel) if len(nel) == 3 else workloads.mbb2d(*nel)
+    E = torch.as_tensor(wl["E"], device="cuda")
+    _, k64, s64, fe64 = setup_problem(wl, 3, "fp64", tol=1e-8)
+    U64, _ = fe64.solve(E)
+    _, k32, s32, fe32 = setup_problem(wl, 3, "mixed", tol=1e-8)
+    U32, res = fe32.solve(E)
+    assert s32.last_info["status"] == "PF_OK"
+    assert true_res(k32, U32, fe32.rhs) < 2e-8
+    c64, c32 = float(torch.dot(fe64.rhs, U64)), float(torch.dot(fe32.rhs, U32))
+    assert abs(c32 - c64) < 1e-6 * abs(c64)
+    assert s32.last_info["iterations"] <= 2 * s64.last_info["iterations"] + 5
+
+
+def test_warm_start_and_cg():
+    wl = workloads.cantilever3d(16, 8, 8)
+    E = torch.as_tensor(wl["E"], device="cuda")
+    _, kern, sol, fe = setup_problem(wl, 2, tol=1e-9)
+    U1, _ = fe.solve(E)
+    it1 = sol.last_info["iterations"]
+    U2, _ = fe.solve(E)  # warm start from the converged solution
+    assert sol.last_info["iterations"] <= 1
+    _, kcg, scg, fcg = setup_problem(wl, 2, tol=1e-9, maxiter=5000, solver="cg")
+    Ucg, res = fcg.solve(E)
+    assert scg.last_info["status"] == "PF_OK" and res < 2e-9
+    assert rel(Ucg.cpu().numpy(), U1.cpu().numpy()) < 1e-7
+    assert it1 < scg.last_info["iterations"]
+
+
+def test_status_not_converged():
+    wl = workloads.cantilever3d(16, 8, 8)
+    _, kern, sol, fe = setup_problem(wl, 2, tol=1e-12, maxiter=3)
+    U, res = fe.solve(torch.as_tensor(wl["E"], device="cuda"))
+    assert sol.last_info["status"] == "PF_NOT_CONVERGED"
+    assert sol.last_info["iterations"] == 3 and res > 1e-12
+
+
+def test_status_nonfinite_input():
+    wl = workloads.cantilever3d(16, 8, 8)
+    _, kern, sol, fe = setup_problem(wl, 2)
+    fe.rhs[5] = float("nan")
+    sol.solve(fe.rhs, rho=torch.as_tensor(wl["E"], device="cuda"), use_last=False)
+    assert sol.last_info["status"] == "PF_NONFINITE"
+
+
+def test_status_breakdown_on_zero_operator():
+    wl = workloads.cantilever3d(8, 4, 4)
+    _, kern, sol, fe = setup_problem(wl, 1, solver="cg")
+    kern.reset()  # no constraints, and a zero stiffness: p.Kp = 0
+    sol.solve(fe.rhs, rho=torch.zeros(8 * 4 * 4, dtype=torch.float64, device="cuda"), use_last=False)
+    assert sol.last_info["status"] == "PF_BREAKDOWN"
+
+
+def test_bad_level_count_is_rejected():
+    from pyfantom_b200._lib import PFError
+    wl = workloads.cantilever3d(12, 8, 8)
+    _, kern, sol, fe = setup_problem(wl, 3)
+    with pytest.raises(PFError):
+        fe.solve(torch.as_tensor(wl["E"], device="cuda"))
+
+
+def _mbb_problem(solver="mg"):
+    from pyfantom_b200.CUDA import (CG, FiniteElement, MinimumCompliance, MultiGrid, OC, StructuredFilter2D,
+                                    StructuredMesh2D, StructuredStiffnessKernel)
+    from pyfantom_b200.physics import LinearElasticity
+    wl = workloads.mbb2d(120, 40)
+    mesh = StructuredMesh2D(120, 40, 120, 40, physics=LinearElasticity(E=1.0, nu=0.3))
+    kern = StructuredStiffnessKernel(mesh)
+    sol = MultiGrid(mesh, kern, maxiter=2000, tol=1e-11, n_smooth=2, omega=0.6, n_level=3)
+    fe = FiniteElement(mesh, kern, sol)
+    left = torch.as_tensor(wl["left_nodes"], device="cuda")
+    fe.add_dirichlet_boundary_condition(node_ids=left, dofs=np.array([[1, 0]]), rhs=0.0)
+    fe.add_dirichlet_boundary_condition(node_ids=np.array([wl["br_node"]]), dofs=np.array([[0, 1]]), rhs=0.0)
+    fe.add_point_forces(forces=np.array([[0.0, -1.0]]), node_ids=np.array([wl["tl_node"]]))
+    filt = StructuredFilter2D(mesh, 1.5)
+    prob = MinimumCompliance(fe, filt, E_mul=[1.0], void=1e-9, penalty=3.0, volume_fraction=[0.5], heavyside=False)
+    return wl, prob, fe
+
+
+def test_mbb_setup_matches_reference(golden):
+    g = golden("mbb")
+    wl, prob, fe = _mbb_problem()
+    assert np.array_equal(np.nonzero(fe.kernel.constraints.cpu().numpy())[0], g["cons"])
+    assert np.array_equal(fe.rhs.cpu().numpy(), g["rhs"])
+
+
+def test_mbb_simp_trajectory_matches_reference(golden):
+    from pyfantom_b200.CUDA import OC
+    g = golden("mbb")
+    wl, prob, fe = _mbb_problem()
+    oc = OC(prob, move=0.2)
+    f = [float(prob.f())]
+    for _ in range(50):
+        oc.iter()
+        f.append(float(prob.f()))
+    f = np.array(f)
+    assert abs(f[0] - g["f"][0]) < 1e-9 * g["f"][0]
+    assert np.abs(f - g["f"]).max() / g["f"].min() < 1e-6
+    assert np.abs(prob.get_desvars().cpu().numpy() - g["x50"]).max() < 1e-5
+    ka = json.load(open(os.path.join(GOLDEN, "known_answers.json")))["mbb_120x40"]
+    assert f[50] == pytest.approx(ka["f_iter50"], rel=1e-6)
+
+
+def test_sensitivity_matches_reference(golden):
+    from pyfantom_b200.CUDA import (FiniteElement, MinimumCompliance, MultiGrid, StructuredFilter3D, StructuredMesh3D,
+                                    StructuredStiffnessKernel)
+    from pyfantom_b200.physics import LinearElasticity
+    g = golden("sensitivity")
+    nel = tuple(int(v) for v in g["nel"])
+    wl = workloads.bridge3d(*nel, seed=3)
+    mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
+    kern = StructuredStiffnessKernel(mesh)
+    sol = MultiGrid(mesh, kern, maxiter=1000, tol=1e-12, n_smooth=2, omega=0.6, n_level=1)
+    fe = FiniteElement(mesh, kern, sol)
+    kern.add_constraints(torch.as_tensor(wl["fixed_dofs"], device="cuda"))
+    fe.rhs.copy_(torch.as_tensor(g["rhs"], device="cuda"))
+    prob = MinimumCompliance(fe, StructuredFilter3D(mesh, 2.5), E_mul=[1.0], void=1e-9, penalty=3.0,
+                             volume_fraction=[0.2], heavyside=False)
+    prob.set_desvars(torch.as_tensor(g["x"], device="cuda"))
+    assert abs(float(prob.f()) - float(g["f"])) < 1e-9 * abs(float(g["f"]))
+    assert rel(prob.nabla_f().cpu().numpy(), g["df"]) < 1e-8
