@@ -1,0 +1,431 @@
+#!/usr/bin/env python
+"""Benchmark: MGCG solves/s of the structured SIMP elasticity solve, one JSON line.
+
+Workload (default ``cantilever_96x48x48``): 96x48x48 H8 cantilever, 698,691 DOF, E0=1,
+Emin=1e-9, nu=0.3, penal=3, densities seeded uniform(0.001,1) Gaussian-smoothed (sigma=2);
+plain FP64 MultiGrid-preconditioned CG, 4 coarse levels, 2 pre/post damped-Jacobi sweeps
+(omega=0.6, reference adaptive schedule), relative residual 1e-8, cold start (x0 = 0).
+One step = one complete solve including the hierarchy setup (the densities change every
+SIMP iteration, so the hierarchy is rebuilt every solve, as in the reference).
+
+Arms
+  default          this library on N GPUs (one process per GPU, replicas: a solve does not
+                   shard; ranks run independent solves, ``scaling: weak``).
+  --impl reference the reference algorithm on the host CPU: the C/OpenMP restatement of the
+                   reference MultiGrid solve (all host threads), same workload and metric.
+
+Timing: W untimed warm-up solves, then K solves, each bracketed by CUDA events on the
+solve stream with a 512 MB L2 flush before each; max over ranks.  ``e2e`` repeats the
+measurement through the public API with the loads and densities in pinned host memory
+(host->device copies and the device->host copy of U inside the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "cantilever_96x48x48": dict(nel=(96, 48, 48), n_level=4),
+    "cantilever_192x96x96": dict(nel=(192, 96, 96), n_level=5),
+    "cantilever_256x128x128": dict(nel=(256, 128, 128), n_level=5),
+}
+METRIC = "MGCG solves/sec (rel-res 1e-8)"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# -----------------------------------------------------------------------------------------
+# clocks sampler
+# -----------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = list(csv.reader(io.StringIO(open(self.f.name).read())))
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -----------------------------------------------------------------------------------------
+# our arm
+# -----------------------------------------------------------------------------------------
+def build_problem(nel, n_level, precision="fp64", tol=1e-8):
+    import torch
+    from pyfantom_b200 import workloads
+    from pyfantom_b200.CUDA import FiniteElement, MultiGrid, StructuredMesh3D, StructuredStiffnessKernel
+    from pyfantom_b200.physics import LinearElasticity
+    wl = workloads.cantilever3d(*nel)
+    mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
+    kern = StructuredStiffnessKernel(mesh)
+    sol = MultiGrid(mesh, kern, maxiter=1000, tol=tol, n_smooth=2, omega=0.6, n_level=n_level, precision=precision)
+    fe = FiniteElement(mesh, kern, sol)
+    fe.add_dirichlet_boundary_condition(node_ids=torch.as_tensor(wl["fixed_nodes"], device="cuda"), rhs=0.0)
+    fe.add_point_forces(forces=wl["load_forces"], node_ids=torch.as_tensor(wl["load_nodes"], device="cuda"))
+    E = torch.as_tensor(wl["E"], device="cuda")
+    return wl, mesh, kern, sol, fe, E
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from pyfantom_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    lib = _lib.load()
+    spec = WORKLOADS[args.workload]
+    nel, nl = spec["nel"], spec["n_level"]
+    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, args.precision)
+    D, Ne = kern.shape[0], int(np.prod(nel))
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def solve_once():
+        kern.set_rho(E)
+        return sol.solve(fe.rhs, use_last=False)
+
+    for _ in range(args.warmup):
+        U, res = solve_once()
+    torch.cuda.synchronize()
+    iters = sol.last_info["iterations"]
+    status = sol.last_info["status"]
+    compliance = float(torch.dot(fe.rhs, U))
+
+    clocks = Clocks()
+    if rank == 0:
+        clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.pf_launch_count()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        U, res = solve_once()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    launches = lib.pf_launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    clk = clocks.stop() if rank == 0 else None
+
+    # ---- end to end through the public API with host buffers --------------------------
+    rhs_h = torch.from_numpy(fe.rhs.cpu().numpy()).pin_memory()
+    E_h = torch.from_numpy(wl["E"]).pin_memory()
+    U_h = torch.empty(D, dtype=torch.float64).pin_memory()
+    E_dev = torch.empty(Ne, dtype=torch.float64, device="cuda")
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fe.rhs.copy_(rhs_h, non_blocking=True)
+        E_dev.copy_(E_h, non_blocking=True)
+        fe.solver.last_x0 = None  # every timed solve starts from x0 = 0
+        U2, _ = fe.solve(E_dev)
+        U_h.copy_(U2, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_max = float(te.item())
+
+    # ---- roofline of the dominant kernel: fine FP64 matvec, timed live in one solve ----
+    lib.pf_mg_set_profiling(sol._mg, 20000)
+    flush.fill_(1.0)
+    solve_once()
+    import ctypes
+    ms, n_l, byts = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+    lib.pf_mg_profile(sol._mg, ctypes.byref(ms), ctypes.byref(n_l), ctypes.byref(byts))
+    lib.pf_mg_set_profiling(sol._mg, 0)
+    avg_us = ms.value / max(n_l.value, 1) * 1e3
+    achieved = byts.value / max(ms.value, 1e-12) / 1e6  # GB/s
+    hbm, peak_kind = peaks()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+            "kernel": "k_matvec_h8<double> (fine-level stiffness matvec with fused epilogues)",
+            "launches_in_solve": int(n_l.value), "avg_launch_us": round(avg_us, 2),
+            "algorithmic_bytes_per_launch": round(byts.value / max(n_l.value, 1))}
+    prof_path = os.path.join(ROOT, "profiles", "matvec_h8_traffic.json")
+    if os.path.exists(prof_path):
+        tr = json.load(open(prof_path)).get(args.workload)
+        if tr:
+            roof["traffic"] = tr.get("dram_bytes_per_launch")
+            roof["traffic_source"] = tr.get("source")
+
+    result = {
+        "metric": METRIC, "value": round(world * args.steps / (max_ms / 1e3), 4), "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 outer / f32 V-cycle",
+        "data": "synthetic (seeded smoothed-random densities, cantilever loads)",
+        "config": {"workload": args.workload, "nel": list(nel), "dof": D, "n_level": nl, "n_smooth": 2,
+                   "omega": 0.6, "tol": 1e-8, "precision": args.precision, "start": "cold (x0 = 0)",
+                   "l2": "512 MB L2 flush before every timed solve", "parallelism": f"replicas x{world}"},
+        "pcg_iterations": iters, "status": status, "compliance": compliance,
+        "e2e": {"value": round(world * args.steps / (e2e_max / 1e3), 4), "unit": "solves/s",
+                "h2d_bytes_per_step": int(8 * (D + Ne)), "d2h_bytes_per_step": int(8 * D)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+    }
+    if rank == 0:
+        result["clocks"] = clk
+    return result, (wl, mesh)
+
+
+def extras(args):
+    """Secondary measurements on one GPU: mixed-precision form at the same workload, and the
+    fine matvec at 256x128x128 (HBM-resident) in FP64 and FP32."""
+    import torch
+    out = {}
+    spec = WORKLOADS[args.workload]
+    wl, mesh, kern, sol, fe, E = build_problem(spec["nel"], spec["n_level"], "mixed")
+    kern.set_rho(E)
+    for _ in range(2):
+        U, _ = sol.solve(fe.rhs, use_last=False)
+    torch.cuda.synchronize()
+    t = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        U, _ = sol.solve(fe.rhs, use_last=False)
+        e1.record()
+        e1.synchronize()
+        t.append(e0.elapsed_time(e1))
+    r = fe.rhs - kern.dot(U)
+    out["mixed_precision"] = {"solves_per_s": round(1e3 / statistics.median(t), 3),
+                              "pcg_iterations": sol.last_info["iterations"],
+                              "true_rel_residual": float(torch.linalg.norm(r) / torch.linalg.norm(fe.rhs)),
+                              "compliance": float(torch.dot(fe.rhs, U))}
+    del wl, mesh, kern, sol, fe, E
+    # fine matvec at 256x128x128, L2 flushed between launches
+    from pyfantom_b200 import _lib
+    from pyfantom_b200 import workloads
+    from pyfantom_b200.CUDA import StructuredMesh3D, StructuredStiffnessKernel
+    from pyfantom_b200.physics import LinearElasticity
+    nel = (256, 128, 128)
+    w5 = workloads.cantilever3d(*nel)
+    mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
+    kern = StructuredStiffnessKernel(mesh)
+    kern.add_constraints(torch.as_tensor(w5["fixed_dofs"], device="cuda"))
+    D, Ne, Nn = kern.shape[0], int(np.prod(nel)), kern.n_nodes
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    lib = _lib.load()
+    for prec, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        Et = torch.as_tensor(w5["E"], device="cuda").to(dt)
+        u = torch.randn(D, dtype=dt, device="cuda")
+        y = torch.empty_like(u)
+        f = lib.pf_matvec_f64 if dt == torch.float64 else lib.pf_matvec_f32
+        ts = []
+        for i in range(8):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(f(kern._op, _lib.ptr(Et), _lib.ptr(u), _lib.ptr(kern.node_mask), _lib.ptr(y), _lib.stream()))
+            e1.record()
+            e1.synchronize()
+            if i >= 2:
+                ts.append(e0.elapsed_time(e1))
+        ms = statistics.median(ts)
+        sz = 4 if dt == torch.float32 else 8
+        byts = 2 * D * sz + Ne * sz + Nn
+        out[f"matvec_256x128x128_{prec}"] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts,
+                                             "GB_per_s": round(byts / ms / 1e6, 1),
+                                             "dof_matvecs_per_s": round(D / ms * 1e3, 1)}
+    return out
+
+
+def probe_matvec(args):
+    """Time the fine-level matvec alone (FP64 and FP32, L2 flushed before every launch)."""
+    import torch
+    from pyfantom_b200 import _lib, workloads
+    from pyfantom_b200.CUDA import StructuredMesh3D, StructuredStiffnessKernel
+    from pyfantom_b200.physics import LinearElasticity
+    nel = WORKLOADS[args.workload]["nel"]
+    w = workloads.cantilever3d(*nel)
+    mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
+    kern = StructuredStiffnessKernel(mesh)
+    kern.add_constraints(torch.as_tensor(w["fixed_dofs"], device="cuda"))
+    D, Ne, Nn = kern.shape[0], int(np.prod(nel)), kern.n_nodes
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    lib = _lib.load()
+    out = {"probe": "matvec", "workload": args.workload}
+    for prec, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        Et = torch.as_tensor(w["E"], device="cuda").to(dt)
+        u = torch.randn(D, dtype=dt, device="cuda")
+        y = torch.empty_like(u)
+        f = lib.pf_matvec_f64 if dt == torch.float64 else lib.pf_matvec_f32
+        ts = []
+        for i in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(f(kern._op, _lib.ptr(Et), _lib.ptr(u), _lib.ptr(kern.node_mask), _lib.ptr(y), _lib.stream()))
+            e1.record()
+            e1.synchronize()
+            if i >= args.warmup:
+                ts.append(e0.elapsed_time(e1))
+        ms = statistics.median(ts)
+        sz = 4 if dt == torch.float32 else 8
+        byts = 2 * D * sz + Ne * sz + Nn
+        out[prec] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts, "GB_per_s": round(byts / ms / 1e6, 1)}
+    return out
+
+
+# -----------------------------------------------------------------------------------------
+# reference arm and CPU baseline: the oracle (C/OpenMP restatement of the reference solve)
+# -----------------------------------------------------------------------------------------
+def cpu_solve(nel, n_level):
+    from oracle import oracle as O
+    from pyfantom_b200 import workloads
+    from pyfantom_b200.physics import LinearElasticity
+    from pyfantom_b200.geom import _unit_element
+    wl = workloads.cantilever3d(*nel)
+    K0 = LinearElasticity(E=1.0, nu=0.3).K(_unit_element((1.0, 1.0, 1.0)))
+    t = time.perf_counter()
+    x, it, res, st = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=n_level, n_smooth=2,
+                                  omega=0.6, tol=1e-8)
+    return time.perf_counter() - t, it, float(wl["rhs"] @ x), O.num_threads()
+
+
+def run_reference(args):
+    spec = WORKLOADS[args.workload]
+    warm = min(args.warmup, 1)  # compiled C: one untimed solve warms caches and page tables
+    for _ in range(warm):
+        cpu_solve(spec["nel"], spec["n_level"])
+    ts = []
+    for _ in range(args.steps):
+        dt, it, c, threads = cpu_solve(spec["nel"], spec["n_level"])
+        ts.append(dt)
+    total = sum(ts)
+    v = args.steps / total
+    return {
+        "metric": METRIC, "value": round(v, 5), "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": warm, "ms_per_step": round(total / args.steps * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, "nel": list(spec["nel"]), "n_level": spec["n_level"], "tol": 1e-8},
+        "pcg_iterations": it, "compliance": c,
+        "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} complete solves of the workload on the host CPU"},
+        "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cantilever_96x48x48", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--probe", choices=["matvec"], default=None,
+                    help="only time the fine matvec (FP64 and FP32) at the workload size (for ncu captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    import torch
+    if args.probe == "matvec":
+        print(json.dumps(probe_matvec(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    result, _ = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_extras:
+        result["forms"] = extras(args)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        spec = WORKLOADS[args.workload]
+        if spec["nel"] == (96, 48, 48):
+            dt, it, c, threads = cpu_solve(spec["nel"], spec["n_level"])
+            result["cpu_baseline"] = {"value": round(1.0 / dt, 5), "unit": "solves/s", "cores": threads, "kind": "port",
+                                      "sample": "one complete solve of the workload (C/OpenMP oracle, all host threads)",
+                                      "pcg_iterations": it, "compliance": c}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -49,6 +49,7 @@ typedef struct pf_grid {
 
 /* ---- library ------------------------------------------------------------------------ */
 int pf_version(void);                     /* 100*major + minor */
+unsigned long long pf_launch_count(void);  /* kernels launched by this library so far */
 const char* pf_last_error(void);          /* message of the last failure on this thread */
 const char* pf_status_string(int status); /* static name of a status code */
 
@@ -128,6 +129,11 @@ int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega, void* stre
  * Blocks the calling thread until the solve ends; info is filled on return. */
 int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, int maxiter,
                 pf_solve_info* info, void* stream);
+/* Diagnostics: time every fine-level matvec launch of the following solves with CUDA
+ * events (at most max_launches per solve; 0 disables), and read the last solve's totals:
+ * device milliseconds, launches, and algorithmic bytes (each operand counted once). */
+int pf_mg_set_profiling(pf_mg* mg, int max_launches);
+int pf_mg_profile(const pf_mg* mg, double* h_ms, long long* h_launches, double* h_bytes);
 /* Number of doubles of device workspace pf_cg_solve needs for `op`. */
 size_t pf_cg_workspace_size(const pf_op* op);
 /* Unpreconditioned CG on K(E) x = b (the matrix-free CG of _solvers.py:22-132).  `work`

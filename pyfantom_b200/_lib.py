@@ -59,6 +59,9 @@ _SZ = ctypes.c_size_t
 # name -> (restype, argtypes); every exported symbol of include/pyfantom_b200.h
 SIGNATURES = {
     "pf_version": (_I, []),
+    "pf_launch_count": (ctypes.c_ulonglong, []),
+    "pf_mg_set_profiling": (_I, [_P, _I]),
+    "pf_mg_profile": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_LL), ctypes.POINTER(_D)]),
     "pf_last_error": (ctypes.c_char_p, []),
     "pf_status_string": (ctypes.c_char_p, [_I]),
     "pf_op_create": (_I, [ctypes.POINTER(pf_grid), _P, ctypes.POINTER(_P)]),

@@ -1,4 +1,5 @@
 // C ABI: library info, errors, element operator objects and single-kernel entry points.
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 #include <vector>
@@ -10,6 +11,10 @@
 namespace pf {
 
 static thread_local char g_err[1024] = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -51,6 +56,8 @@ struct pf_op_holder {
 };
 
 extern "C" int pf_version(void) { return 100; }
+
+extern "C" unsigned long long pf_launch_count(void) { return pf::launch_count(); }
 
 extern "C" const char* pf_last_error(void) { return pf::g_err; }
 

@@ -157,4 +157,8 @@ __device__ __forceinline__ T epi_omega(const Epi<T>& e) {
 
 constexpr int kNumSM = 148;
 
+// number of kernels this library has launched since it was loaded (diagnostics)
+void count_launch(unsigned long long n = 1);
+unsigned long long launch_count();
+
 }  // namespace pf

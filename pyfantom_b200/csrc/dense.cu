@@ -182,18 +182,27 @@ void dense_free(Dense* d) {
 int dense_factor_invert(Dense* d, double beta, cudaStream_t st) {
     const int np = d->np, nt = np / TB;
     PF_CUDA(cudaMemsetAsync(d->fail, 0, sizeof(int), st));
+    pf::count_launch();
     k_pad_diag<<<(np + 255) / 256, 256, 0, st>>>(d->M, d->n, np, beta);
     for (int p = 0; p < nt; p++) {
+        pf::count_launch();
         k_potrf_tile<<<1, dim3(TB, TB), 0, st>>>(d->M, np, p, d->fail);
         if (p + 1 < nt) {
+            pf::count_launch();
             k_trsm<<<nt - p - 1, TB, 0, st>>>(d->M, np, p);
             const int T = nt - p - 1;
+            pf::count_launch();
             k_syrk<<<T * (T + 1) / 2, dim3(TB, TB), 0, st>>>(d->M, np, p);
         }
     }
     PF_CUDA(cudaMemsetAsync(d->Linv, 0, (size_t)np * np * sizeof(double), st));
+    pf::count_launch();
     k_trtri_tiles<<<nt, TB, 0, st>>>(d->M, d->Linv, np);
-    for (int i = 1; i < nt; i++) k_linv_row<<<i, dim3(TB, TB), 0, st>>>(d->M, d->Linv, np, i);
+    for (int i = 1; i < nt; i++) {
+        pf::count_launch();
+        k_linv_row<<<i, dim3(TB, TB), 0, st>>>(d->M, d->Linv, np, i);
+    }
+    pf::count_launch();
     k_ainv<<<dim3(nt, nt), dim3(TB, TB), 0, st>>>(d->Linv, d->Ainv, np, nt);
     PF_LAUNCH_CHECK("coarse factorisation launch");
     return PF_OK;
@@ -201,6 +210,7 @@ int dense_factor_invert(Dense* d, double beta, cudaStream_t st) {
 
 template <typename T>
 int dense_solve(const Dense* d, const T* b, T* x, const int* skip, cudaStream_t st) {
+    pf::count_launch();
     k_dense_matvec<T><<<(d->n + 7) / 8, 256, 0, st>>>(d->Ainv, d->np, d->n, b, x, skip);
     PF_LAUNCH_CHECK("coarse solve launch");
     return PF_OK;

@@ -85,46 +85,86 @@ struct H8Blk {
     T b[8][3][3];
 };
 
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Pipelined x-march.  Step s (element layer ie = ix0-1+s):
+//   1. cp.async the node plane ie+2 into plane buffer s&1 (last read in step s-1) and this
+//      thread's epilogue operands for its node of plane ie into its private slots;
+//   2. forward stages of the plane ie+1 face (buffer (s+1)&1), element operator, inverse
+//      stages, node sums inside the warp (shuffles), exchange row sums in s_x[s&1];
+//   3. wait for this thread's copies, zero the constrained components it copied,
+//      __syncthreads (the only barrier of the step);
+//   4. owners finish their node of plane ie and apply the epilogue.
 template <typename T, typename TE, int TY>
 __global__ void __launch_bounds__((TY + 1) * 32)
     k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
                 const uint8_t* __restrict__ mask, const H8Blk<T> blk, Epi<T> epi) {
     constexpr int NW = TY + 1;
     constexpr int NT = NW * 32;
-    constexpr int PR = TY + 2, PC = 33;
-    __shared__ T s_u[2][3][PR][PC];
-    __shared__ T s_x[3][NW][32];
+    constexpr int PR = TY + 2, PC = 33, NPE = PR * PC;
+    constexpr int NQ = (NPE + NT - 1) / NT;  // plane entries per thread
+    constexpr int NSLOT = 6;                 // u (identity rows), b, x, dinv, xadd, dot_a
+    __shared__ __align__(16) T s_u[2][3][PR][PC];
+    __shared__ T s_x[2][3][NW][32];
+    __shared__ __align__(16) T s_ep[NSLOT][3][NT];
     __shared__ double s_red[NW];
-
+    __shared__ T s_blk[8 * 9];
     if (epi.skip && *epi.skip) return;
     const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     const int kz0 = blockIdx.x * 31, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
     const int je = jy0 - 1 + w, ke = kz0 - 1 + l;
     const int jn = jy0 + w, kn = kz0 + l;
     const bool owner = (w < TY) && (l < 31) && (jn < ny) && (kn < nz);
     const bool col_ok = (je >= 0) && (je < NY) && (ke >= 0) && (ke < NZ);
     const T wgt = epi_omega(epi);
+    const int mode = epi.mode;
+    const bool need_b = mode != PF_EPI_STORE, need_d = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
+    const bool need_xa = mode == PF_EPI_JACOBI_ADD, need_dot = epi.dot_partial != nullptr;
     double dot = 0.0;
+    constexpr int TB_ = (int)sizeof(T);
 
-    auto load_plane = [&](int p, int buf) {
-        for (int idx = threadIdx.x; idx < PR * PC; idx += NT) {
-            const int r = idx / PC, c = idx - r * PC;
-            const int j = jy0 - 1 + r, k = kz0 - 1 + c;
-            T v0 = T(0), v1 = T(0), v2 = T(0);
-            if (p >= 0 && p < nx && j >= 0 && j < ny && k >= 0 && k < nz) {
-                const long long n = (long long)k + (long long)nz * (p + (long long)nx * j);
-                const uint8_t m = mask ? mask[n] : (uint8_t)0;
-                v0 = (m & 1) ? T(0) : u[3 * n];
-                v1 = (m & 2) ? T(0) : u[3 * n + 1];
-                v2 = (m & 4) ? T(0) : u[3 * n + 2];
+    // issue the copies of plane p into buffer buf; returns the masks of the entries issued
+    auto issue_plane = [&](int p, int buf, uint8_t* mq) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const int idx = tid + q * NT;
+            mq[q] = 0;
+            if (idx < NPE) {
+                const int r = idx / PC, c = idx - r * PC;
+                const int j = jy0 - 1 + r, k = kz0 - 1 + c;
+                if (p >= 0 && p < nx && j >= 0 && j < ny && k >= 0 && k < nz) {
+                    const long long n = (long long)k + (long long)nz * (p + (long long)nx * j);
+                    mq[q] = mask ? mask[n] : (uint8_t)0;
+#pragma unroll
+                    for (int d = 0; d < 3; d++) cp_async(&s_u[buf][d][r][c], u + 3 * n + d, TB_);
+                } else {
+#pragma unroll
+                    for (int d = 0; d < 3; d++) s_u[buf][d][r][c] = T(0);
+                }
             }
-            s_u[buf][0][r][c] = v0;
-            s_u[buf][1][r][c] = v1;
-            s_u[buf][2][r][c] = v2;
         }
     };
-    // forward y/z stages on this thread's face: g[comp][mb][mc]
+    auto fix_plane = [&](int buf, const uint8_t* mq) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const int idx = tid + q * NT;
+            if (idx < NPE && mq[q]) {
+                const int r = idx / PC, c = idx - r * PC;
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+                    if (mq[q] & (1 << d)) s_u[buf][d][r][c] = T(0);
+            }
+        }
+    };
     auto face = [&](int buf, T g[3][2][2]) {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -137,66 +177,98 @@ __global__ void __launch_bounds__((TY + 1) * 32)
             g[c][1][1] = d1 - d0;
         }
     };
+    auto epi_copy = [&](int slot, const T* src, long long n) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) cp_async(&s_ep[slot][d][tid], src + 3 * n + d, TB_);
+    };
 
-    load_plane(ix0 - 1, 0);
+    if (tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
+    // the coefficients are re-read from shared memory at every use (volatile) rather than
+    // held in 72 (FP32) / 144 (FP64) registers for the whole kernel
+    const volatile T* vb = s_blk;
+#define BK(p, i, j) vb[(p) * 9 + (i) * 3 + (j)]
+    // prologue: planes ix0-1 (buffer 0) and ix0 (buffer 1)
+    uint8_t mq[NQ];
+    issue_plane(ix0 - 1, 0, mq);
+    cp_async_commit();
+    cp_async_wait_all();
+    fix_plane(0, mq);
+    issue_plane(ix0, 1, mq);
+    cp_async_commit();
+    cp_async_wait_all();
+    fix_plane(1, mq);
     __syncthreads();
     T glo[3][2][2], carry[3][2][2];
     face(0, glo);
+    __syncthreads();  // step 0 refills buffer 0: every warp must have read it first
 #pragma unroll
     for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int a = 0; a < 2; a++)
 #pragma unroll
             for (int b = 0; b < 2; b++) carry[c][a][b] = T(0);
+    T e_next = T(0);
+    if (col_ok && ix0 - 1 >= 0 && ix0 - 1 < NX) e_next = (T)E[((long long)(ix0 - 1) * NY + je) * NZ + ke];
 
-    int buf = 0;
     for (int s = 0; s <= CXc; s++) {
         const int ie = ix0 - 1 + s;
-        const int nb = buf ^ 1;
-        load_plane(ie + 1, nb);
-        __syncthreads();
-        T ghi[3][2][2];
-        face(nb, ghi);
-        T e = T(0);
-        if (col_ok && ie >= 0 && ie < NX) e = (T)E[((long long)ie * NY + je) * NZ + ke];
-        // x stage (with the density folded in): v[c][ma][mb][mc]
-        T v[3][2][2][2];
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int mb = 0; mb < 2; mb++)
-#pragma unroll
-                for (int mc = 0; mc < 2; mc++) {
-                    const T t = e * ghi[c][mb][mc];
-                    v[c][0][mb][mc] = fma(e, glo[c][mb][mc], t);
-                    v[c][1][mb][mc] = fma(-e, glo[c][mb][mc], t);
-                }
-        // class blocks: component c of class p sits in mode p ^ e_c
-        T wv[3][2][2][2];
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            const int px = p & 1, py = (p >> 1) & 1, pz = (p >> 2) & 1;
-            const T i0 = v[0][px ^ 1][py][pz], i1 = v[1][px][py ^ 1][pz], i2 = v[2][px][py][pz ^ 1];
-            wv[0][px ^ 1][py][pz] = fma(blk.b[p][0][0], i0, fma(blk.b[p][0][1], i1, blk.b[p][0][2] * i2));
-            wv[1][px][py ^ 1][pz] = fma(blk.b[p][1][0], i0, fma(blk.b[p][1][1], i1, blk.b[p][1][2] * i2));
-            wv[2][px][py][pz ^ 1] = fma(blk.b[p][2][0], i0, fma(blk.b[p][2][1], i1, blk.b[p][2][2] * i2));
+        const int cur = (s + 1) & 1;
+        // 1. asynchronous copies
+        issue_plane(ie + 2, s & 1, mq);
+        const bool out_now = owner && s >= 1 && ie < nx;
+        long long n_out = 0;
+        uint8_t m_out = 0;
+        if (out_now) {
+            n_out = (long long)kn + (long long)nz * (ie + (long long)nx * jn);
+            m_out = mask ? mask[n_out] : (uint8_t)0;
+            if (m_out) epi_copy(0, u, n_out);
+            if (need_b) epi_copy(1, epi.b, n_out);
+            if (mode == PF_EPI_JACOBI || need_xa) epi_copy(2, epi.x, n_out);
+            if (need_d) epi_copy(3, epi.dinv, n_out);
+            if (need_xa) epi_copy(4, epi.xadd, n_out);
+            if (need_dot) epi_copy(5, epi.dot_a, n_out);
         }
-        // inverse x stage; the lower face completes with the previous layer's upper face
+        cp_async_commit();
+        const T e = e_next;
+        e_next = (col_ok && ie + 1 >= 0 && ie + 1 < NX) ? (T)E[((long long)(ie + 1) * NY + je) * NZ + ke] : T(0);
+        // 2. element operator
+        T ghi[3][2][2];
+        face(cur, ghi);
+        // Element operator by (y,z) parity: the pair of classes p = (0,py,pz), (1,py,pz)
+        // reads and writes exactly the modes (c=0: py,pz), (c=1: py^1,pz), (c=2: py,pz^1),
+        // so x stage, two 3x3 blocks and the inverse x stage complete per pair.
+        T G[3][2][2];
+#pragma unroll
+        for (int pyz = 0; pyz < 4; pyz++) {
+            const int py = pyz & 1, pz = pyz >> 1;
+            const int p0 = 2 * py + 4 * pz, p1 = p0 + 1;
+            // x stage of the three (component, y-mode, z-mode) slots of this pair
+            const T h0 = e * ghi[0][py][pz], h1 = e * ghi[1][py ^ 1][pz], h2 = e * ghi[2][py][pz ^ 1];
+            const T a0 = fma(e, glo[0][py][pz], h0), b0 = fma(-e, glo[0][py][pz], h0);
+            const T a1 = fma(e, glo[1][py ^ 1][pz], h1), b1 = fma(-e, glo[1][py ^ 1][pz], h1);
+            const T a2 = fma(e, glo[2][py][pz ^ 1], h2), b2 = fma(-e, glo[2][py][pz ^ 1], h2);
+            // class p0 (px = 0): comp 0 in x-mode 1, comps 1, 2 in x-mode 0
+            const T o00 = fma(BK(p0, 0, 0), b0, fma(BK(p0, 0, 1), a1, BK(p0, 0, 2) * a2));
+            const T o01 = fma(BK(p0, 1, 0), b0, fma(BK(p0, 1, 1), a1, BK(p0, 1, 2) * a2));
+            const T o02 = fma(BK(p0, 2, 0), b0, fma(BK(p0, 2, 1), a1, BK(p0, 2, 2) * a2));
+            // class p1 (px = 1): comp 0 in x-mode 0, comps 1, 2 in x-mode 1
+            const T o10 = fma(BK(p1, 0, 0), a0, fma(BK(p1, 0, 1), b1, BK(p1, 0, 2) * b2));
+            const T o11 = fma(BK(p1, 1, 0), a0, fma(BK(p1, 1, 1), b1, BK(p1, 1, 2) * b2));
+            const T o12 = fma(BK(p1, 2, 0), a0, fma(BK(p1, 2, 1), b1, BK(p1, 2, 2) * b2));
+            // inverse x stage: (x-mode 0, x-mode 1) -> lower face w0 - w1, upper face w0 + w1
+            G[0][py][pz] = (o10 - o00) + carry[0][py][pz];
+            carry[0][py][pz] = o10 + o00;
+            G[1][py ^ 1][pz] = (o01 - o11) + carry[1][py ^ 1][pz];
+            carry[1][py ^ 1][pz] = o01 + o11;
+            G[2][py][pz ^ 1] = (o02 - o12) + carry[2][py][pz ^ 1];
+            carry[2][py][pz ^ 1] = o02 + o12;
+        }
+        // inverse z then y stage -> corner contributions t[c][b][cz]
         T t[3][2][2];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            T G[2][2];
-#pragma unroll
-            for (int mb = 0; mb < 2; mb++)
-#pragma unroll
-                for (int mc = 0; mc < 2; mc++) {
-                    const T w0 = wv[c][0][mb][mc], w1 = wv[c][1][mb][mc];
-                    G[mb][mc] = (w0 - w1) + carry[c][mb][mc];
-                    carry[c][mb][mc] = w0 + w1;
-                }
-            // inverse z then y stage -> corner contributions t[c][b][cz]
-            const T q00 = G[0][0] - G[0][1], q01 = G[0][0] + G[0][1];
-            const T q10 = G[1][0] - G[1][1], q11 = G[1][0] + G[1][1];
+            const T q00 = G[c][0][0] - G[c][0][1], q01 = G[c][0][0] + G[c][0][1];
+            const T q10 = G[c][1][0] - G[c][1][1], q11 = G[c][1][0] + G[c][1][1];
             t[c][0][0] = q00 - q10;
             t[c][0][1] = q01 - q11;
             t[c][1][0] = q00 + q10;
@@ -208,20 +280,28 @@ __global__ void __launch_bounds__((TY + 1) * 32)
         for (int c = 0; c < 3; c++) {
             P1[c] = t[c][1][1] + __shfl_down_sync(0xffffffffu, t[c][1][0], 1);
             const T P0 = t[c][0][1] + __shfl_down_sync(0xffffffffu, t[c][0][0], 1);
-            s_x[c][w][l] = P0;
+            s_x[s & 1][c][w][l] = P0;
         }
+        // 3. copies landed, constrained components zeroed, one barrier
+        cp_async_wait_all();
+        fix_plane(s & 1, mq);
         __syncthreads();
-        if (owner && s >= 1 && ie < nx) {
-            const long long n = (long long)kn + (long long)nz * (ie + (long long)nx * jn);
-            const uint8_t m = mask ? mask[n] : (uint8_t)0;
+        // 4. owners finish their node of plane ie
+        if (out_now) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                T y = P1[c] + s_x[c][w + 1][l];
-                if (m & (1 << c)) y = u[3 * n + c];
-                const long long g = 3 * n + c;
-                const T o = epi_apply(epi, g, y, wgt);
-                epi.out[g] = o;
-                if (epi.dot_partial) dot += (double)epi.dot_a[g] * (double)(epi.dot_of_y ? y : o);
+                T y = P1[c] + s_x[s & 1][c][w + 1][l];
+                if (m_out & (1 << c)) y = s_ep[0][c][tid];
+                T o = y;
+                if (mode == PF_EPI_RESID) {
+                    o = s_ep[1][c][tid] - y;
+                } else if (mode == PF_EPI_JACOBI) {
+                    o = s_ep[2][c][tid] + wgt * s_ep[3][c][tid] * (s_ep[1][c][tid] - y);
+                } else if (mode == PF_EPI_JACOBI_ADD) {
+                    o = s_ep[4][c][tid] + s_ep[2][c][tid] + wgt * s_ep[3][c][tid] * (s_ep[1][c][tid] - y);
+                }
+                epi.out[3 * n_out + c] = o;
+                if (need_dot) dot += (double)s_ep[5][c][tid] * (double)(epi.dot_of_y ? y : o);
             }
         }
 #pragma unroll
@@ -230,8 +310,8 @@ __global__ void __launch_bounds__((TY + 1) * 32)
             for (int a = 0; a < 2; a++)
 #pragma unroll
                 for (int b = 0; b < 2; b++) glo[c][a][b] = ghi[c][a][b];
-        buf = nb;
     }
+#undef BK
     if (epi.dot_partial) {
         const double sblk = block_sum<NT>(dot, s_red);
         if (threadIdx.x == 0)
@@ -346,10 +426,12 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
         dim3 grid;
         int cx;
         h8_launch_dims(g, TY, &grid, &cx);
+        pf::count_launch();
         k_matvec_h8<T, TE, TY><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
                                                              make_blk<T>(op), epi);
     } else {
         const long long nb = q4_num_blocks(g);
+        pf::count_launch();
         k_matvec_q4<T, TE><<<(unsigned)nb, 256, 0, st>>>(g.nel[0], g.nel[1], u, E, mask, make_q4k<T>(op), epi);
     }
     PF_LAUNCH_CHECK("fine matvec launch");
@@ -408,6 +490,7 @@ int launch_diagonal(const Op* op, const double* E, const uint8_t* mask, T* diag,
     KDiag kd;
     const int nd = (g.dim == 3 ? 8 : 4) * g.dim;
     for (int i = 0; i < nd; i++) kd.d[i] = op->K0[i * nd + i];
+    pf::count_launch();
     k_diagonal<T><<<(unsigned)((g.n_nodes + 255) / 256), 256, 0, st>>>(g, E, mask, kd, diag);
     PF_LAUNCH_CHECK("diagonal launch");
     return PF_OK;
@@ -498,6 +581,7 @@ __global__ void k_sens_q4(int NX, int NY, const double* __restrict__ U, const Q4
 int launch_sensitivity(const Op* op, const double* U, double* dk, cudaStream_t st) {
     const Grid& g = op->grid;
     const unsigned nb = (unsigned)((g.n_elem + 255) / 256);
+    pf::count_launch();
     if (g.dim == 3)
         k_sens_h8<<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], U, make_blk<double>(op), dk);
     else
@@ -517,6 +601,7 @@ __global__ void k_pack_mask(long long n_nodes, int dof, const uint8_t* __restric
 
 int launch_pack_mask(const Op* op, const uint8_t* con, uint8_t* mask, cudaStream_t st) {
     const Grid& g = op->grid;
+    pf::count_launch();
     k_pack_mask<<<(unsigned)((g.n_nodes + 255) / 256), 256, 0, st>>>(g.n_nodes, g.dof, con, mask);
     PF_LAUNCH_CHECK("pack mask launch");
     return PF_OK;

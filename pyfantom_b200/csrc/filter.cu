@@ -73,6 +73,7 @@ static int launch_filter(const pf_filter* f, int mode, const double* x, double* 
     const unsigned nb = (unsigned)((g.n_elem + 255) / 256);
     const size_t sm = (size_t)f->n_taps * (sizeof(double) + g.dim * sizeof(int));
     const int nz = g.dim == 3 ? g.nel[2] : 1;
+    count_launch();
 #define PF_FILTER_CASE(D, M) \
     k_filter<D, M><<<nb, 256, sm, st>>>(g.nel[0], g.nel[1], nz, f->n_taps, f->d_off, f->d_w, f->d_norm, x, y)
     if (g.dim == 3) {

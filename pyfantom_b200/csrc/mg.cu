@@ -71,6 +71,13 @@ struct pf_mg {
     cudaEvent_t ev[6] = {};  // 0,1 setup; 2 solve start; 3,4 chunk polls; 5 solve end
     bool ready = false;
     double setup_ms = 0.0;
+    // optional CUDA-event timing of every fine-level matvec launch of a solve
+    int profile = 0;
+    std::vector<cudaEvent_t> pev;  // pairs (start, end)
+    std::vector<double> pbytes;    // algorithmic bytes of each recorded launch
+    int pn = 0;
+    double prof_ms = 0.0, prof_bytes = 0.0;
+    long long prof_launches = 0;
 };
 
 namespace pf {
@@ -249,14 +256,41 @@ static unsigned vec_blocks(long long n) {
 // ---------------------------------------------------------------------------------------
 // level operators
 // ---------------------------------------------------------------------------------------
+// algorithmic bytes of one fine matvec launch: u, E, mask and out once each, plus the
+// epilogue operands (b, dinv, xadd) and a dot operand other than u
+template <typename T>
+static double fine_mv_bytes(const pf_mg* mg, const T* u, const Epi<T>& e) {
+    const Grid& g = mg->op->grid;
+    const double D = (double)g.n_nodes * g.dof, tb = sizeof(T);
+    double b = 2.0 * D * tb + (double)g.n_elem * tb + (mg->mask ? (double)g.n_nodes : 0.0);
+    if (e.mode == PF_EPI_RESID) b += D * tb;
+    if (e.mode == PF_EPI_JACOBI) b += 2.0 * D * tb;
+    if (e.mode == PF_EPI_JACOBI_ADD) b += 3.0 * D * tb;
+    if (e.dot_partial && (const void*)e.dot_a != (const void*)u) b += D * tb;
+    return b;
+}
+
+template <typename T>
+static int fine_mv(pf_mg* mg, const T* u, const Epi<T>& epi, cudaStream_t st) {
+    const bool rec = mg->profile && mg->pn < (int)mg->pev.size() / 2;
+    if (rec) PF_CUDA(cudaEventRecord(mg->pev[2 * mg->pn], st));
+    int s;
+    if constexpr (sizeof(T) == 8)
+        s = launch_fine_matvec<double, double>(mg->op, mg->E, u, mg->mask, epi, st);
+    else
+        s = launch_fine_matvec<float, float>(mg->op, mg->Ef, u, mg->mask, epi, st);
+    if (s) return s;
+    if (rec) {
+        PF_CUDA(cudaEventRecord(mg->pev[2 * mg->pn + 1], st));
+        mg->pbytes[mg->pn] = fine_mv_bytes<T>(mg, u, epi);
+        mg->pn++;
+    }
+    return PF_OK;
+}
+
 template <typename T>
 static int level_matvec(pf_mg* mg, int l, const T* u, const Epi<T>& epi, cudaStream_t st) {
-    if (l == 0) {
-        if constexpr (sizeof(T) == 8)
-            return launch_fine_matvec<double, double>(mg->op, mg->E, u, mg->mask, epi, st);
-        else
-            return launch_fine_matvec<float, float>(mg->op, mg->Ef, u, mg->mask, epi, st);
-    }
+    if (l == 0) return fine_mv<T>(mg, u, epi, st);
     if constexpr (sizeof(T) == 8)
         return launch_stencil_matvec<double>(mg->L[l].g, mg->L[l].A64, u, epi, st);
     else
@@ -300,6 +334,7 @@ static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, 
     T* X = (T*)L.x;
     T* Tb = (T*)L.t;
     int s;
+    pf::count_launch();
     k_jacobi0<T><<<vec_blocks(L.ndof), kRedThreads, 0, st>>>(L.ndof, b, dinv, omega, scale, X, skip);
     PF_LAUNCH_CHECK("jacobi0 launch");
     for (int k = 1; k < mg->cfg.n_smooth; k++) {
@@ -456,6 +491,7 @@ extern "C" int pf_mg_destroy(pf_mg* mg) {
     cudaDeviceSynchronize();
     for (int i = 0; i < 6; i++)
         if (mg->ev[i]) cudaEventDestroy(mg->ev[i]);
+    for (cudaEvent_t e : mg->pev) cudaEventDestroy(e);
     mg_free(mg);
     delete mg;
     return PF_OK;
@@ -477,10 +513,12 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
     // level 0: inverse diagonal
     if (mg->fp32) {
         if ((s = launch_diagonal<float>(mg->op, E, node_mask, (float*)L0.dinv, st))) return s;
+        pf::count_launch();
         k_recip<float><<<vec_blocks(L0.ndof), kRedThreads, 0, st>>>(L0.ndof, (float*)L0.dinv);
         if ((s = launch_d2f(g.n_elem, E, mg->Ef, st))) return s;
     } else {
         if ((s = launch_diagonal<double>(mg->op, E, node_mask, (double*)L0.dinv, st))) return s;
+        pf::count_launch();
         k_recip<double><<<vec_blocks(L0.ndof), kRedThreads, 0, st>>>(L0.ndof, (double*)L0.dinv);
     }
     PF_LAUNCH_CHECK("recip launch");
@@ -533,6 +571,7 @@ __global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_o
 
 static int init_state(pf_mg* mg, double tol, int maxiter, double omega, cudaStream_t st) {
     const double min_omega = fmax(mg->cfg.omega / 2.0, mg->cfg.min_omega);
+    pf::count_launch();
     k_init_state<<<1, 1, 0, st>>>(mg->st, tol, maxiter, min_omega, mg->cfg.omega - min_omega, omega);
     PF_LAUNCH_CHECK("state init");
     return PF_OK;
@@ -546,9 +585,11 @@ extern "C" int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega,
     if ((s = init_state(mg, 0.0, 1, omega, st))) return s;
     const long long n = mg->L[0].ndof;
     if (mg->fp32) {
+        pf::count_launch();
         k_d2f_skip<<<vec_blocks(n), kRedThreads, 0, st>>>(n, r, (float*)mg->L[0].b, nullptr);
         float* res;
         if ((s = vcycle<float>(mg, 0, (const float*)mg->L[0].b, &res, nullptr, nullptr, st))) return s;
+        pf::count_launch();
         k_f2d<<<vec_blocks(n), kRedThreads, 0, st>>>(n, res, z);
     } else {
         double* res;
@@ -564,9 +605,11 @@ static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaSt
     const long long n = mg->L[0].ndof;
     int s;
     if (mg->fp32) {
+        pf::count_launch();
         k_d2f_skip<<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->r, (float*)mg->L[0].b, &mg->st->done);
         float* res;
         if ((s = vcycle<float>(mg, 0, (const float*)mg->L[0].b, &res, nullptr, nullptr, st))) return s;
+        pf::count_launch();
         k_dot_partial<float><<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->r, res, mg->partials, &mg->st->done);
         PF_LAUNCH_CHECK("dot launch");
         *z_out = res;
@@ -582,6 +625,7 @@ static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaSt
 
 static int update_p(pf_mg* mg, const void* z, int init, cudaStream_t st) {
     const long long n = mg->L[0].ndof;
+    pf::count_launch();
     if (mg->fp32)
         k_pcg_p<float><<<vec_blocks(n), kRedThreads, 0, st>>>(n, (const float*)z, mg->p, mg->st, init);
     else
@@ -599,14 +643,18 @@ static int pcg_iteration(pf_mg* mg, double* x, cudaStream_t st) {
     e.dot_partial = mg->partials;
     e.dot_a = mg->p;
     e.dot_of_y = 1;
-    if ((s = launch_fine_matvec<double, double>(mg->op, mg->E, mg->p, mg->mask, e, st))) return s;
+    if ((s = fine_mv<double>(mg, mg->p, e, st))) return s;
+    pf::count_launch();
     k_pcg_alpha<<<1, kRedThreads, 0, st>>>(mg->partials, fine_matvec_num_blocks(mg->op, 0), mg->st);
+    pf::count_launch();
     k_pcg_xr<<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->p, mg->q, x, mg->r, mg->st, mg->partials);
+    pf::count_launch();
     k_pcg_check<<<1, kRedThreads, 0, st>>>(mg->partials, vec_blocks(n), mg->st);
     PF_LAUNCH_CHECK("pcg launch");
     const void* z;
     long long np;
     if ((s = precondition(mg, &z, &np, st))) return s;
+    pf::count_launch();
     k_pcg_beta<<<1, kRedThreads, 0, st>>>(mg->partials, np, mg->st);
     PF_LAUNCH_CHECK("beta launch");
     return update_p(mg, z, 0, st);
@@ -621,16 +669,19 @@ extern "C" int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, do
     const long long n = mg->L[0].ndof;
     int s;
     if ((s = init_state(mg, tol, maxiter, 0.0, st))) return s;
+    mg->pn = 0;
     PF_CUDA(cudaEventRecord(mg->ev[2], st));
     // r = b - K x (or b with x = 0), ||b||
     if (use_x0) {
         Epi<double> e = make_epi<double>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, mg->r, nullptr, 1.0, nullptr);
-        if ((s = launch_fine_matvec<double, double>(mg->op, mg->E, x, mg->mask, e, st))) return s;
+        if ((s = fine_mv<double>(mg, x, e, st))) return s;
     } else {
         PF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
         PF_CUDA(cudaMemcpyAsync(mg->r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
+    pf::count_launch();
     k_dot_partial<double><<<vec_blocks(n), kRedThreads, 0, st>>>(n, b, b, mg->partials, nullptr);
+    pf::count_launch();
     k_pcg_normb<<<1, kRedThreads, 0, st>>>(mg->partials, vec_blocks(n), mg->st);
     PF_LAUNCH_CHECK("pcg start");
     if (maxiter == 0) {
@@ -650,6 +701,7 @@ extern "C" int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, do
     const void* z;
     long long np;
     if ((s = precondition(mg, &z, &np, st))) return s;
+    pf::count_launch();
     k_pcg_rho0<<<1, kRedThreads, 0, st>>>(mg->partials, np, mg->st);
     if ((s = update_p(mg, z, 1, st))) return s;
     // iterate in chunks, polling the completion flag of the previous chunk
@@ -689,6 +741,17 @@ extern "C" int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, do
         info->setup_ms = setup_ms;
         info->solve_ms = solve_ms;
     }
+    if (mg->profile) {
+        mg->prof_ms = 0.0;
+        mg->prof_bytes = 0.0;
+        mg->prof_launches = mg->pn;
+        for (int i = 0; i < mg->pn; i++) {
+            float ms = 0.f;
+            PF_CUDA(cudaEventElapsedTime(&ms, mg->pev[2 * i], mg->pev[2 * i + 1]));
+            mg->prof_ms += ms;
+            mg->prof_bytes += mg->pbytes[i];
+        }
+    }
     int fpiv = 0;
     PF_CUDA(cudaMemcpy(&fpiv, mg->dense.fail, sizeof(int), cudaMemcpyDeviceToHost));
     if (fpiv) {
@@ -721,6 +784,7 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
     double *r = work, *p = work + n, *q = work + 2 * n, *partials = work + 3 * n;
     PcgState* S = (PcgState*)(partials + npart);
     const int* skip = &S->done;
+    pf::count_launch();
     k_init_state<<<1, 1, 0, st>>>(S, tol, maxiter, 0.0, 0.0, 0.0);
     if (use_x0) {
         Epi<double> e = make_epi<double>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, r, nullptr, 1.0, nullptr);
@@ -731,10 +795,15 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
         PF_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     const unsigned vb = vec_blocks(n);
+    pf::count_launch();
     k_dot_partial<double><<<vb, kRedThreads, 0, st>>>(n, b, b, partials, nullptr);
+    pf::count_launch();
     k_pcg_normb<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+    pf::count_launch();
     k_dot_partial<double><<<vb, kRedThreads, 0, st>>>(n, r, r, partials, skip);
+    pf::count_launch();
     k_pcg_rho0<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+    pf::count_launch();
     k_pcg_p<double><<<vb, kRedThreads, 0, st>>>(n, r, p, S, 1);
     PF_LAUNCH_CHECK("cg start");
     cudaEvent_t e0, e1;
@@ -753,10 +822,15 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
             e.dot_of_y = 1;
             int s = launch_fine_matvec<double, double>(op, E, p, node_mask, e, st);
             if (s) return s;
+            pf::count_launch();
             k_pcg_alpha<<<1, kRedThreads, 0, st>>>(partials, nbm, S);
+            pf::count_launch();
             k_pcg_xr<<<vb, kRedThreads, 0, st>>>(n, p, q, x, r, S, partials);
+            pf::count_launch();
             k_pcg_check<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+            pf::count_launch();
             k_pcg_beta<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+            pf::count_launch();
             k_pcg_p<double><<<vb, kRedThreads, 0, st>>>(n, r, p, S, 0);
         }
         PF_LAUNCH_CHECK("cg iteration");
@@ -779,5 +853,33 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
         info->setup_ms = 0.0;
         info->solve_ms = ms;
     }
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// profiling of the fine-level matvec inside a solve
+// ---------------------------------------------------------------------------------------
+extern "C" int pf_mg_set_profiling(pf_mg* mg, int max_launches) {
+    if (!mg || max_launches < 0) return fail(PF_BAD_ARG, "pf_mg_set_profiling: bad argument");
+    PF_CUDA(cudaDeviceSynchronize());
+    for (cudaEvent_t e : mg->pev) cudaEventDestroy(e);
+    mg->pev.clear();
+    mg->pbytes.clear();
+    mg->profile = max_launches > 0;
+    mg->pn = 0;
+    for (int i = 0; i < 2 * max_launches; i++) {
+        cudaEvent_t e;
+        PF_CUDA(cudaEventCreate(&e));
+        mg->pev.push_back(e);
+    }
+    mg->pbytes.assign(max_launches, 0.0);
+    return PF_OK;
+}
+
+extern "C" int pf_mg_profile(const pf_mg* mg, double* h_ms, long long* h_launches, double* h_bytes) {
+    if (!mg || !h_ms || !h_launches || !h_bytes) return fail(PF_BAD_ARG, "pf_mg_profile: NULL argument");
+    *h_ms = mg->prof_ms;
+    *h_launches = mg->prof_launches;
+    *h_bytes = mg->prof_bytes;
     return PF_OK;
 }

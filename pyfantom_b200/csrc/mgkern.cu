@@ -133,6 +133,7 @@ template <typename TI, typename TO>
 int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st) {
     const Grid gc = coarse_grid(gf);
     const unsigned nb = (unsigned)((gc.n_nodes + 255) / 256);
+    pf::count_launch();
     if (gf.dim == 3)
         k_restrict<3, TI, TO><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vf, vc, skip);
     else
@@ -144,6 +145,7 @@ template <typename T>
 int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st) {
     const Grid gc = coarse_grid(gf);
     const unsigned nb = (unsigned)((gf.n_nodes + 255) / 256);
+    pf::count_launch();
     if (gf.dim == 3)
         k_prolong<3, T><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vc, vf, skip);
     else
@@ -205,6 +207,7 @@ __global__ void __launch_bounds__(256) k_stencil_matvec(GridDev<DIM> g, const T*
 template <typename T>
 int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st) {
     const unsigned nb = (unsigned)((g.n_nodes + 255) / 256);
+    pf::count_launch();
     if (g.dim == 3)
         k_stencil_matvec<3, T><<<nb, 256, 0, st>>>(gdev<3>(g), A, u, epi);
     else
@@ -394,6 +397,7 @@ void galerkin_child_matrices(int dim, const double* K0, double* Kc) {
 int launch_coarse_flags(const Grid& gf, const uint8_t* mask, uint8_t* elem_flag, uint8_t* node_flag, cudaStream_t st) {
     const Grid gc = coarse_grid(gf);
     const unsigned nb = (unsigned)((gc.n_nodes + 255) / 256);
+    pf::count_launch();
     if (gf.dim == 3)
         k_coarse_flags<3><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), mask, elem_flag, node_flag);
     else
@@ -408,6 +412,7 @@ int launch_galerkin_l0(const Grid& gf, const double* E, const uint8_t* mask, con
     const int NB = gf.dim == 3 ? 27 : 9;
     const long long n = gc.n_nodes * NB;
     const unsigned nb = (unsigned)((n + 127) / 128);
+    pf::count_launch();
     if (gf.dim == 3)
         k_galerkin_l0<3><<<nb, 128, 0, st>>>(gdev<3>(gf), gdev<3>(gc), E, mask, elem_flag, node_flag, K0_dev, Kc_dev, A);
     else
@@ -503,6 +508,7 @@ int launch_galerkin_l1p(const Grid& gf, const double* Af, double* Ac, cudaStream
     const Grid gc = coarse_grid(gf);
     const int NB = gf.dim == 3 ? 27 : 9;
     const unsigned nb = (unsigned)((gc.n_nodes * NB + 127) / 128);
+    pf::count_launch();
     if (gf.dim == 3)
         k_galerkin_l1p<3><<<nb, 128, 0, st>>>(gdev<3>(gf), gdev<3>(gc), Af, Ac);
     else
@@ -527,6 +533,7 @@ __global__ void k_stencil_dinv(long long N, int dim, const double* __restrict__ 
 template <typename T>
 int launch_stencil_dinv(const Grid& g, const double* A, T* dinv, cudaStream_t st) {
     const long long n = g.n_nodes * g.dim;
+    pf::count_launch();
     k_stencil_dinv<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g.n_nodes, g.dim, A, dinv);
     PF_LAUNCH_CHECK("stencil dinv launch");
     return PF_OK;
@@ -554,6 +561,7 @@ __global__ void k_stencil_to_dense(GridDev<DIM> g, const double* __restrict__ A,
 int launch_stencil_to_dense(const Grid& g, const double* A, double* M, long long ld, cudaStream_t st) {
     const int NB = g.dim == 3 ? 27 : 9;
     const long long n = g.n_nodes * NB * g.dim * g.dim;
+    pf::count_launch();
     if (g.dim == 3)
         k_stencil_to_dense<3><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gdev<3>(g), A, M, ld);
     else
@@ -570,6 +578,7 @@ int launch_d2f(long long n, const double* a, float* b, cudaStream_t st) {
     long long nb = (n + 255) / 256;
     if (nb > 4 * kNumSM * 8) nb = 4 * kNumSM * 8;
     if (nb < 1) nb = 1;
+    pf::count_launch();
     k_d2f<<<(unsigned)nb, 256, 0, st>>>(n, a, b);
     PF_LAUNCH_CHECK("d2f launch");
     return PF_OK;

@@ -248,13 +248,19 @@ int oc_update(long long n, const double* x, const double* df, const double* dg, 
     double* ocp = work;
     double* partials = work + n;
     OcState* S = reinterpret_cast<OcState*>(partials + (size_t)nb * kOcTree);
+    pf::count_launch();
     k_oc_prep<<<nb, kRT, 0, st>>>(n, x, df, dg, ocp, partials);
+    pf::count_launch();
     k_oc_init<<<1, kRT, 0, st>>>(partials, nb, S);
     for (int p = 0; p < kOcPasses; p++) {
+        pf::count_launch();
         k_oc_eval<<<nb, kRT, 0, st>>>(n, x, ocp, dg, move, S, partials);
+        pf::count_launch();
         k_oc_step<<<1, 32, 0, st>>>(partials, nb, vf, S);
     }
+    pf::count_launch();
     k_oc_write<<<nb, kRT, 0, st>>>(n, x, ocp, move, S, x_new, partials);
+    pf::count_launch();
     k_oc_change<<<1, kRT, 0, st>>>(partials, nb, S);
     PF_LAUNCH_CHECK("oc launch");
     if (h_out) {
@@ -277,6 +283,7 @@ extern "C" int pf_penalize_f64(long long n, const double* rho, const pf_simp_par
                                void* stream) {
     if (n < 0 || !rho || !p || (!E && !dE)) return fail(PF_BAD_ARG, "pf_penalize_f64: bad argument");
     if (n == 0) return PF_OK;
+    pf::count_launch();
     k_penalize<<<grid_for(n), kRT, 0, as_stream(stream)>>>(n, rho, *p, E, dE);
     PF_LAUNCH_CHECK("penalize launch");
     return PF_OK;
@@ -285,6 +292,7 @@ extern "C" int pf_penalize_f64(long long n, const double* rho, const pf_simp_par
 extern "C" int pf_mul_f64(long long n, const double* a, const double* b, double* out, void* stream) {
     if (n < 0 || !a || !b || !out) return fail(PF_BAD_ARG, "pf_mul_f64: bad argument");
     if (n == 0) return PF_OK;
+    pf::count_launch();
     k_mul<<<grid_for(n), kRT, 0, as_stream(stream)>>>(n, a, b, out);
     PF_LAUNCH_CHECK("mul launch");
     return PF_OK;
@@ -296,7 +304,9 @@ extern "C" int pf_dot_f64(long long n, const double* a, const double* b, double*
     if (n < 0 || !a || !b || !result || !work) return fail(PF_BAD_ARG, "pf_dot_f64: bad argument");
     cudaStream_t st = as_stream(stream);
     const unsigned nb = grid_for(n < 1 ? 1 : n);
+    pf::count_launch();
     k_dot_part<<<nb, kRT, 0, st>>>(n, a, b, work);
+    pf::count_launch();
     k_sum_to<<<1, kRT, 0, st>>>(work, (int)nb, result);
     PF_LAUNCH_CHECK("dot launch");
     return PF_OK;

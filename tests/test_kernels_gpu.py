@@ -110,6 +110,27 @@ def test_matvec_vs_oracle_shapes(lib, nel):
     assert rel(y32, O.matvec(nel, K0, E.astype(np.float32), u.astype(np.float32), cons)) < 2e-5
 
 
+@pytest.mark.parametrize("nel", [(96, 48, 48), (64, 64, 64), (48, 96, 40)])
+def test_matvec_large_and_repeatable(lib, nel):
+    """Full-size grids (many blocks per SM, every tile and chunk edge) in FP64 and FP32, and
+    bitwise run-to-run equality over repeated launches (catches shared-memory races)."""
+    rng = np.random.default_rng(99)
+    op = Op(lib, nel)
+    E = rng.uniform(1e-3, 1.0, int(np.prod(nel)))
+    u = rng.standard_normal(op.ndof)
+    cons = np.arange(0, 3 * (nel[2] + 1) * (nel[0] + 1), 1)  # the y = 0 face region, all DOFs
+    ref = O.matvec(nel, op.K0, E, u, cons)
+    y0 = op.matvec(E, u, cons)
+    assert rel(y0, ref) < 1e-12
+    for _ in range(10):
+        assert np.array_equal(op.matvec(E, u, cons), y0)
+    y32 = op.matvec(E.astype(np.float32), u.astype(np.float32), cons, fp32=True)
+    ref32 = O.matvec(nel, op.K0, E.astype(np.float32), u.astype(np.float32), cons)
+    assert rel(y32, ref32) < 2e-5
+    for _ in range(10):
+        assert np.array_equal(op.matvec(E.astype(np.float32), u.astype(np.float32), cons, fp32=True), y32)
+
+
 def test_matvec_anisotropic_element(lib):
     K0 = unit_K0(3, nu=0.25, h=(1.0, 0.5, 2.0))
     nel = (6, 10, 4)

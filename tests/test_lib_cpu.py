@@ -13,7 +13,7 @@ HEADER = os.path.join(ROOT, "include", "pyfantom_b200.h")
 
 def declared_symbols():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|size_t|const char\*)\s+(pf_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|const char\*|unsigned long long)\s+(pf_\w+)\s*\(", src, flags=re.M)))
 
 
 def test_header_declares_entry_points():

@@ -206,3 +206,25 @@ def test_sensitivity_matches_reference(golden):
     prob.set_desvars(torch.as_tensor(g["x"], device="cuda"))
     assert abs(float(prob.f()) - float(g["f"])) < 1e-9 * abs(float(g["f"]))
     assert rel(prob.nabla_f().cpu().numpy(), g["df"]) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_full_size_cantilever_matches_reference(precision):
+    """96x48x48 cantilever (698,691 DOF), 4 levels, tol 1e-8: the reference MultiGrid takes
+    83 PCG iterations and reaches compliance 7.472352867980982 (tests/golden/known_answers.json
+    records the reference run).  The FP64 drop-in must match the iteration count (+-1); both
+    forms must reach a true FP64 residual near 1e-8 and the compliance within 1e-6."""
+    wl = workloads.cantilever3d(96, 48, 48)
+    _, kern, sol, fe = setup_problem(wl, 4, precision, tol=1e-8, maxiter=1000)
+    for _ in range(2):  # repeated solves must agree bitwise (FP64) / stay converged (mixed)
+        U, res = fe.solve(torch.as_tensor(wl["E"], device="cuda"))
+        sol.last_x0 = None
+        info = sol.last_info
+        assert info["status"] == "PF_OK"
+        if precision == "fp64":
+            assert abs(info["iterations"] - 83) <= 1
+        else:
+            assert info["iterations"] <= 100
+        assert true_res(kern, U, fe.rhs) < 1.5e-8
+        c = float(torch.dot(fe.rhs, U))
+        assert abs(c - 7.472352867980982) < 1e-6 * 7.472352867980982
