@@ -14,6 +14,7 @@ static thread_local char g_err[1024] = "";
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launch(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {

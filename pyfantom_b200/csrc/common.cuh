@@ -159,6 +159,7 @@ constexpr int kNumSM = 148;
 
 // number of kernels this library has launched since it was loaded (diagnostics)
 void count_launch(unsigned long long n = 1);
+void uncount_launch(unsigned long long n);
 unsigned long long launch_count();
 
 }  // namespace pf

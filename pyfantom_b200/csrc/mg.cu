@@ -72,6 +72,16 @@ struct pf_mg {
     bool ready = false;
     double setup_ms = 0.0;
     // optional CUDA-event timing of every fine-level matvec launch of a solve
+    // internal copies that keep the pointers captured in the CUDA graphs valid across solves
+    double* Eint = nullptr;
+    double* bi = nullptr;
+    double* xi = nullptr;
+    cudaStream_t cs = nullptr;        // private stream the solve runs (and is captured) on
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraphExec_t g_start[2] = {nullptr, nullptr};  // start sequence, without / with x0
+    cudaGraphExec_t g_chunk = nullptr;                // check_every PCG iterations
+    unsigned long long g_start_nodes[2] = {0, 0}, g_chunk_nodes = 0;
+    const uint8_t* g_mask = nullptr;  // node mask the graphs were captured with
     int profile = 0;
     std::vector<cudaEvent_t> pev;  // pairs (start, end)
     std::vector<double> pbytes;    // algorithmic bytes of each recorded launch
@@ -387,8 +397,14 @@ static void mg_free(pf_mg* mg) {
     }
     dense_free(&mg->dense);
     for (void* p : {(void*)mg->K0_dev, (void*)mg->Kc_dev, (void*)mg->elem_flag, (void*)mg->node_flag, (void*)mg->Ef,
-                    (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st})
+                    (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st,
+                    (void*)mg->Eint, (void*)mg->bi, (void*)mg->xi})
         if (p) cudaFree(p);
+    for (cudaGraphExec_t g : {mg->g_start[0], mg->g_start[1], mg->g_chunk})
+        if (g) cudaGraphExecDestroy(g);
+    if (mg->ev_in) cudaEventDestroy(mg->ev_in);
+    if (mg->ev_out) cudaEventDestroy(mg->ev_out);
+    if (mg->cs) cudaStreamDestroy(mg->cs);
     if (mg->h_snap) cudaFreeHost(mg->h_snap);
 }
 
@@ -466,6 +482,13 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     mg->npartials = np;
     s = s ? s : dalloc((void**)&mg->partials, np * sizeof(double));
     s = s ? s : dalloc((void**)&mg->st, sizeof(PcgState));
+    s = s ? s : dalloc((void**)&mg->Eint, (size_t)g.n_elem * sizeof(double));
+    s = s ? s : dalloc((void**)&mg->bi, n0 * sizeof(double));
+    s = s ? s : dalloc((void**)&mg->xi, n0 * sizeof(double));
+    if (!s && (cudaStreamCreateWithFlags(&mg->cs, cudaStreamNonBlocking) != cudaSuccess ||
+               cudaEventCreateWithFlags(&mg->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+               cudaEventCreateWithFlags(&mg->ev_out, cudaEventDisableTiming) != cudaSuccess))
+        s = fail(PF_CUDA_ERROR, "stream / event creation failed");
     if (!s && cudaMallocHost((void**)&mg->h_snap, 2 * sizeof(PcgState)) != cudaSuccess)
         s = fail(PF_NO_MEMORY, "pinned allocation failed");
     if (!s) {
@@ -503,10 +526,17 @@ extern "C" int pf_mg_destroy(pf_mg* mg) {
 extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask, void* stream) {
     if (!mg || !E) return fail(PF_BAD_ARG, "pf_mg_setup: NULL argument");
     cudaStream_t st = as_stream(stream);
+    PF_CUDA(cudaEventRecord(mg->ev[0], st));
+    PF_CUDA(cudaMemcpyAsync(mg->Eint, E, sizeof(double) * mg->op->grid.n_elem, cudaMemcpyDeviceToDevice, st));
+    E = mg->Eint;
     mg->E = E;
+    if (node_mask != mg->g_mask) {  // graphs bake the mask pointer in: recapture
+        for (cudaGraphExec_t& g : mg->g_start)
+            if (g) cudaGraphExecDestroy(g), g = nullptr;
+        if (mg->g_chunk) cudaGraphExecDestroy(mg->g_chunk), mg->g_chunk = nullptr;
+    }
     mg->mask = node_mask;
     mg->ready = false;
-    PF_CUDA(cudaEventRecord(mg->ev[0], st));
     int s;
     Level& L0 = mg->L[0];
     const Grid& g = mg->op->grid;
@@ -660,78 +690,122 @@ static int pcg_iteration(pf_mg* mg, double* x, cudaStream_t st) {
     return update_p(mg, z, 0, st);
 }
 
-extern "C" int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, int maxiter,
-                           pf_solve_info* info, void* stream) {
-    if (!mg || !b || !x) return fail(PF_BAD_ARG, "pf_mg_solve: NULL argument");
-    if (!mg->ready) return fail(PF_BAD_ARG, "pf_mg_solve: call pf_mg_setup first");
-    if (maxiter < 0) return fail(PF_BAD_ARG, "maxiter must be >= 0");
-    cudaStream_t st = as_stream(stream);
+// Capture the launches `body` issues on the private stream into an executable graph.
+template <typename F>
+static int capture(pf_mg* mg, F body, cudaGraphExec_t* out, unsigned long long* nodes) {
+    const unsigned long long c0 = launch_count();
+    PF_CUDA(cudaStreamBeginCapture(mg->cs, cudaStreamCaptureModeThreadLocal));
+    int s = body(mg->cs);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(mg->cs, &graph);
+    *nodes = launch_count() - c0;
+    uncount_launch(*nodes);  // captured, not launched
+    if (s) {
+        if (graph) cudaGraphDestroy(graph);
+        return s;
+    }
+    if (e != cudaSuccess) return check_cuda(e, "stream capture");
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return check_cuda(e, "graph instantiate");
+    return PF_OK;
+}
+
+// r = b - K x (or b with x = 0), ||b||, z = M r, p = z, rho = r.z
+static int solve_start(pf_mg* mg, int use_x0, cudaStream_t st) {
     const long long n = mg->L[0].ndof;
     int s;
-    if ((s = init_state(mg, tol, maxiter, 0.0, st))) return s;
-    mg->pn = 0;
-    PF_CUDA(cudaEventRecord(mg->ev[2], st));
-    // r = b - K x (or b with x = 0), ||b||
     if (use_x0) {
-        Epi<double> e = make_epi<double>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, mg->r, nullptr, 1.0, nullptr);
-        if ((s = fine_mv<double>(mg, x, e, st))) return s;
+        Epi<double> e = make_epi<double>(PF_EPI_RESID, mg->bi, nullptr, nullptr, nullptr, mg->r, nullptr, 1.0, nullptr);
+        if ((s = fine_mv<double>(mg, mg->xi, e, st))) return s;
     } else {
-        PF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
-        PF_CUDA(cudaMemcpyAsync(mg->r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        PF_CUDA(cudaMemsetAsync(mg->xi, 0, n * sizeof(double), st));
+        PF_CUDA(cudaMemcpyAsync(mg->r, mg->bi, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     pf::count_launch();
-    k_dot_partial<double><<<vec_blocks(n), kRedThreads, 0, st>>>(n, b, b, mg->partials, nullptr);
+    k_dot_partial<double><<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->bi, mg->bi, mg->partials, nullptr);
     pf::count_launch();
     k_pcg_normb<<<1, kRedThreads, 0, st>>>(mg->partials, vec_blocks(n), mg->st);
     PF_LAUNCH_CHECK("pcg start");
-    if (maxiter == 0) {
-        PcgState* h = &mg->h_snap[0];
-        PF_CUDA(cudaMemcpyAsync(h, mg->st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-        PF_CUDA(cudaStreamSynchronize(st));
-        if (info) {
-            info->iterations = 0;
-            info->status = h->done ? h->status : PF_NOT_CONVERGED;
-            info->residual = h->R;
-            info->setup_ms = 0;
-            info->solve_ms = 0;
-        }
-        return PF_OK;
-    }
-    // z = M r, p = z, rho = r.z
     const void* z;
     long long np;
     if ((s = precondition(mg, &z, &np, st))) return s;
     pf::count_launch();
     k_pcg_rho0<<<1, kRedThreads, 0, st>>>(mg->partials, np, mg->st);
-    if ((s = update_p(mg, z, 1, st))) return s;
-    // iterate in chunks, polling the completion flag of the previous chunk
+    return update_p(mg, z, 1, st);
+}
+
+extern "C" int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, int maxiter,
+                           pf_solve_info* info, void* stream) {
+    if (!mg || !b || !x) return fail(PF_BAD_ARG, "pf_mg_solve: NULL argument");
+    if (!mg->ready) return fail(PF_BAD_ARG, "pf_mg_solve: call pf_mg_setup first");
+    if (maxiter < 0) return fail(PF_BAD_ARG, "maxiter must be >= 0");
+    cudaStream_t us = as_stream(stream), cs = mg->cs;
+    const long long n = mg->L[0].ndof;
     const int C = mg->cfg.check_every;
+    const bool graphs = !mg->profile;
+    int s;
+    // the private stream starts after everything already queued on the caller's stream
+    PF_CUDA(cudaEventRecord(mg->ev_in, us));
+    PF_CUDA(cudaStreamWaitEvent(cs, mg->ev_in, 0));
+    if ((s = init_state(mg, tol, maxiter, 0.0, cs))) return s;
+    mg->pn = 0;
+    PF_CUDA(cudaEventRecord(mg->ev[2], cs));
+    PF_CUDA(cudaMemcpyAsync(mg->bi, b, n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    if (use_x0) PF_CUDA(cudaMemcpyAsync(mg->xi, x, n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    const int v = use_x0 ? 1 : 0;
+    if (graphs) {
+        if (!mg->g_start[v] &&
+            (s = capture(mg, [&](cudaStream_t c) { return solve_start(mg, use_x0, c); }, &mg->g_start[v],
+                         &mg->g_start_nodes[v])))
+            return s;
+        PF_CUDA(cudaGraphLaunch(mg->g_start[v], cs));
+        count_launch(mg->g_start_nodes[v]);
+    } else if ((s = solve_start(mg, use_x0, cs))) {
+        return s;
+    }
+    if (graphs && !mg->g_chunk && maxiter > 0) {
+        auto body = [&](cudaStream_t c) {
+            for (int k = 0; k < C; k++) {
+                int r = pcg_iteration(mg, mg->xi, c);
+                if (r) return r;
+            }
+            return (int)PF_OK;
+        };
+        if ((s = capture(mg, body, &mg->g_chunk, &mg->g_chunk_nodes))) return s;
+    }
+    mg->g_mask = mg->mask;
+    // iterate in chunks of C, polling the completion flag of the previous chunk while the
+    // next one is queued; iterations past convergence or maxiter are no-ops on the device
     int queued = 0, chunk = 0;
-    bool finished = false;
-    while (!finished) {
-        const int todo = (maxiter - queued) < C ? (maxiter - queued) : C;
-        for (int k = 0; k < todo; k++)
-            if ((s = pcg_iteration(mg, x, st))) return s;
-        queued += todo;
+    while (queued < maxiter) {
+        if (graphs) {
+            PF_CUDA(cudaGraphLaunch(mg->g_chunk, cs));
+            count_launch(mg->g_chunk_nodes);
+        } else {
+            for (int k = 0; k < C; k++)
+                if ((s = pcg_iteration(mg, mg->xi, cs))) return s;
+        }
+        queued += C;
         const int slot = chunk & 1;
-        PF_CUDA(cudaMemcpyAsync(&mg->h_snap[slot], mg->st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-        PF_CUDA(cudaEventRecord(mg->ev[3 + slot], st));
-        if (queued >= maxiter) break;
+        PF_CUDA(cudaMemcpyAsync(&mg->h_snap[slot], mg->st, sizeof(PcgState), cudaMemcpyDeviceToHost, cs));
+        PF_CUDA(cudaEventRecord(mg->ev[3 + slot], cs));
         if (chunk > 0) {
             const int prev = slot ^ 1;
             PF_CUDA(cudaEventSynchronize(mg->ev[3 + prev]));
-            if (mg->h_snap[prev].done) finished = true;
+            if (mg->h_snap[prev].done) break;
         }
         chunk++;
     }
-    PF_CUDA(cudaStreamSynchronize(st));
+    PF_CUDA(cudaMemcpyAsync(x, mg->xi, n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    PF_CUDA(cudaEventRecord(mg->ev[5], cs));
+    PF_CUDA(cudaEventRecord(mg->ev_out, cs));
+    PF_CUDA(cudaStreamWaitEvent(us, mg->ev_out, 0));
+    PF_CUDA(cudaStreamSynchronize(cs));
     PcgState fin;
     PF_CUDA(cudaMemcpy(&fin, mg->st, sizeof(PcgState), cudaMemcpyDeviceToHost));
-    // the setup events were recorded on the same stream before this call
     float setup_ms = 0.f, solve_ms = 0.f;
     if (cudaEventElapsedTime(&setup_ms, mg->ev[0], mg->ev[1]) != cudaSuccess) setup_ms = 0.f;
-    cudaEventRecord(mg->ev[5], st);
-    cudaEventSynchronize(mg->ev[5]);
     if (cudaEventElapsedTime(&solve_ms, mg->ev[2], mg->ev[5]) != cudaSuccess) solve_ms = 0.f;
     cudaGetLastError();
     if (info) {

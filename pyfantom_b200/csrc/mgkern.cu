@@ -160,25 +160,30 @@ template int launch_prolong<float>(const Grid&, const float*, float*, const int*
 
 // ---------------------------------------------------------------------------------------
 // block-stencil matvec (levels >= 1): y_n = sum_o A[n,o] u_{n+o}
+// A block covers 32 consecutive nodes; warp w gathers the neighbour offsets 3w..3w+2 for
+// all 32 nodes (coalesced reads of the structure-of-arrays coefficients), the per-warp
+// partial sums meet in shared memory and warp 0 adds them in a fixed order and applies the
+// epilogue.  3D: 9 warps x 3 offsets, 2D: 3 warps x 3 offsets.
 // ---------------------------------------------------------------------------------------
 template <int DIM, typename T>
-__global__ void __launch_bounds__(256) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
-                                                         const T* __restrict__ u, Epi<T> epi) {
-    __shared__ double s_red[8];
+__global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
+                                                                        const T* __restrict__ u, Epi<T> epi) {
+    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM, NG = NB / 3;
+    __shared__ T s_part[NG][DIM][32];
     if (epi.skip && *epi.skip) return;
-    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM;
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double dot = 0.0;
-    const T wgt = epi_omega(epi);
-    if (n < g.n_nodes) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const long long n = (long long)blockIdx.x * 32 + l;
+    const long long N = g.n_nodes;
+    const bool valid = n < N;
+    T acc[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; a++) acc[a] = T(0);
+    if (valid) {
         int i, j, k;
         ndec(g, n, i, j, k);
-        T acc[DIM];
 #pragma unroll
-        for (int a = 0; a < DIM; a++) acc[a] = T(0);
-        const long long N = g.n_nodes;
-#pragma unroll
-        for (int o = 0; o < NB; o++) {
+        for (int q = 0; q < 3; q++) {
+            const int o = 3 * w + q;
             const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = DIM == 3 ? o / 9 - 1 : 0;
             if (!nok(g, i + ox, j + oy, k + oz)) continue;
             const long long m = nidx(g, i + ox, j + oy, k + oz);
@@ -190,32 +195,43 @@ __global__ void __launch_bounds__(256) k_stencil_matvec(GridDev<DIM> g, const T*
 #pragma unroll
                 for (int b = 0; b < DIM; b++) acc[a] = fma(A[((long long)(o * BS + a * DIM + b)) * N + n], um[b], acc[a]);
         }
+    }
+#pragma unroll
+    for (int a = 0; a < DIM; a++) s_part[w][a][l] = acc[a];
+    __syncthreads();
+    if (w != 0) return;
+    double dot = 0.0;
+    if (valid) {
+        const T wgt = epi_omega(epi);
 #pragma unroll
         for (int a = 0; a < DIM; a++) {
+            T y = s_part[0][a][l];
+#pragma unroll
+            for (int v = 1; v < NG; v++) y += s_part[v][a][l];
             const long long gi = n * DIM + a;
-            const T o = epi_apply(epi, gi, acc[a], wgt);
+            const T o = epi_apply(epi, gi, y, wgt);
             epi.out[gi] = o;
-            if (epi.dot_partial) dot += (double)epi.dot_a[gi] * (double)(epi.dot_of_y ? acc[a] : o);
+            if (epi.dot_partial) dot += (double)epi.dot_a[gi] * (double)(epi.dot_of_y ? y : o);
         }
     }
     if (epi.dot_partial) {
-        const double s = block_sum<256>(dot, s_red);
-        if (threadIdx.x == 0) epi.dot_partial[blockIdx.x] = s;
+        dot = warp_sum(dot);
+        if (l == 0) epi.dot_partial[blockIdx.x] = dot;
     }
 }
 
 template <typename T>
 int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st) {
-    const unsigned nb = (unsigned)((g.n_nodes + 255) / 256);
+    const unsigned nb = (unsigned)((g.n_nodes + 31) / 32);
     pf::count_launch();
     if (g.dim == 3)
-        k_stencil_matvec<3, T><<<nb, 256, 0, st>>>(gdev<3>(g), A, u, epi);
+        k_stencil_matvec<3, T><<<nb, 288, 0, st>>>(gdev<3>(g), A, u, epi);
     else
-        k_stencil_matvec<2, T><<<nb, 256, 0, st>>>(gdev<2>(g), A, u, epi);
+        k_stencil_matvec<2, T><<<nb, 96, 0, st>>>(gdev<2>(g), A, u, epi);
     PF_LAUNCH_CHECK("stencil matvec launch");
     return PF_OK;
 }
-long long stencil_matvec_num_blocks(const Grid& g) { return (g.n_nodes + 255) / 256; }
+long long stencil_matvec_num_blocks(const Grid& g) { return (g.n_nodes + 31) / 32; }
 template int launch_stencil_matvec<double>(const Grid&, const double*, const double*, const Epi<double>&,
                                            cudaStream_t);
 template int launch_stencil_matvec<float>(const Grid&, const float*, const float*, const Epi<float>&, cudaStream_t);
