@@ -183,6 +183,19 @@ size_t pf_oc_workspace_size(long long n); /* doubles */
 int pf_oc_update_f64(long long n, const double* x, const double* df, const double* dg, double vf,
                      double move, double* x_new, double* work, double* h_out, void* stream);
 
+/* ---- OC update without allocation --------------------------------------------------
+ * No counterpart in the reference.  Same computation and outputs as pf_oc_update_f64,
+ * for callers that cannot allocate device memory where they run the OC step (code being
+ * captured into a CUDA graph, plugins inside a framework that owns the device memory,
+ * latency-bound per-iteration callbacks): the scratch is a static device array of the
+ * library sized for PF_OC_NOALLOC_MAX_ELEMS elements (16.9 MB held by every GPU that loads
+ * the library).  Larger n is rejected with PF_BAD_ARG.  The first call on each device
+ * resolves the array's address (and may load the library's device code): make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU race. */
+#define PF_OC_NOALLOC_MAX_ELEMS 2097152
+int pf_oc_update_noalloc_f64(long long n, const double* x, const double* df, const double* dg, double vf,
+                             double move, double* x_new, double* h_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,7 @@ SIGNATURES = {
     "pf_dot_f64": (_I, [_LL, _P, _P, _P, _P, _P]),
     "pf_oc_workspace_size": (_SZ, [_LL]),
     "pf_oc_update_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
+    "pf_oc_update_noalloc_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P]),
 }
 
 _lib = None
