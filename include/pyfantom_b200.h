@@ -165,6 +165,13 @@ typedef struct pf_simp_params {
 /* E = penalize(rho); dE = penalize_grad(rho) (either output may be NULL) */
 int pf_penalize_f64(long long n, const double* rho, const pf_simp_params* p, double* E, double* dE,
                     void* stream);
+/* Fused adjoint of the compliance (self-adjoint: the adjoint state is -U):
+ * out_e = scale * dE/drho(rho_e) * (-u_e^T K0 u_e), dE/drho as pf_penalize_f64's dE, rho
+ * the filtered densities.  dc/dx = H^T out (pf_filter_adj_f64).  Replaces the chain
+ * process_grad -> penalize_grad -> product of MinimumCompliance._compute
+ * (pyFANTOM/Problem/CUDA/MinimumCompliance.py:428-438) with one kernel. */
+int pf_adjoint_f64(const pf_op* op, const double* U, const double* rho, const pf_simp_params* p,
+                   double scale, double* out, void* stream);
 /* out_e = dE_e * dk_e  (the element factor of the compliance sensitivity) */
 int pf_mul_f64(long long n, const double* a, const double* b, double* out, void* stream);
 

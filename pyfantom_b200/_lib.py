@@ -91,6 +91,7 @@ SIGNATURES = {
     "pf_filter_adj_f64": (_I, [_P, _P, _P, _P]),
     "pf_penalize_f64": (_I, [_LL, _P, ctypes.POINTER(pf_simp_params), _P, _P, _P]),
     "pf_mul_f64": (_I, [_LL, _P, _P, _P, _P]),
+    "pf_adjoint_f64": (_I, [_P, _P, _P, ctypes.POINTER(pf_simp_params), _D, _P, _P]),
     "pf_dot_workspace_size": (_SZ, [_LL]),
     "pf_dot_f64": (_I, [_LL, _P, _P, _P, _P, _P]),
     "pf_oc_workspace_size": (_SZ, [_LL]),

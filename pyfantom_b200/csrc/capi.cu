@@ -180,6 +180,12 @@ extern "C" int pf_sensitivity_f64(const pf_op* op, const double* U, double* dk, 
     return launch_sensitivity(op, U, dk, as_stream(stream));
 }
 
+extern "C" int pf_adjoint_f64(const pf_op* op, const double* U, const double* rho, const pf_simp_params* p,
+                              double scale, double* out, void* stream) {
+    if (!op || !U || !rho || !p || !out) return fail(PF_BAD_ARG, "pf_adjoint_f64: NULL argument");
+    return launch_adjoint(op, U, rho, *p, scale, out, as_stream(stream));
+}
+
 static int even_grid(const pf_grid* fine, Grid* g) {
     int s = validate_grid(fine, g);
     if (s) return s;

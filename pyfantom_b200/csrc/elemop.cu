@@ -498,9 +498,32 @@ int launch_diagonal(const Op* op, const double* E, const uint8_t* mask, T* diag,
 template int launch_diagonal<double>(const Op*, const double*, const uint8_t*, double*, cudaStream_t);
 template int launch_diagonal<float>(const Op*, const double*, const uint8_t*, float*, cudaStream_t);
 
-// dk_e = -(T u_e)^T B (T u_e) (H8) ; dense quadratic form (Q4)
+// Element energy e_e = u_e^T K0 u_e = (T u_e)^T B (T u_e) (H8, Walsh basis) or the dense
+// quadratic form (Q4).  ADJ = false: dk_e = -e_e (reference process_dk, grad.cu:1-16).
+// ADJ = true (the fused adjoint of the compliance): out_e = scale * dE/drho(rho_e) * (-e_e)
+// with the SIMP derivative of the reference's penalize_grad
+// (Problem/CUDA/MinimumCompliance.py:351-367), i.e. the element factor of
+// dc/dx = H^T [dE/drho * (-u_e^T K0 u_e)] before the filter transpose.
+struct AdjArgs {
+    const double* rho;
+    pf_simp_params P;
+    double scale;
+};
+
+__device__ __forceinline__ double simp_grad(double r, const pf_simp_params& P) {
+    double dh = 1.0;
+    if (P.heavyside) {
+        const double den = tanh(P.beta * P.eta) + tanh(P.beta * (1.0 - P.eta));
+        const double t = tanh(P.beta * (r - P.eta));
+        r = (tanh(P.beta * P.eta) + t) / den;
+        dh = P.beta * (1.0 - t * t) / den;
+    }
+    return P.penalty * pow(r, P.penalty - 1.0) * dh * P.E_mul;
+}
+
+template <bool ADJ>
 __global__ void k_sens_h8(int NX, int NY, int NZ, const double* __restrict__ U, const H8Blk<double> blk,
-                          double* __restrict__ dk) {
+                          AdjArgs adj, double* __restrict__ dk) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)NX * NY * NZ) return;
     const int k = (int)(e % NZ), j = (int)((e / NZ) % NY), i = (int)(e / ((long long)NY * NZ));
@@ -553,10 +576,15 @@ __global__ void k_sens_h8(int NX, int NY, int NZ, const double* __restrict__ U, 
         const double o2 = blk.b[p][2][0] * i0 + blk.b[p][2][1] * i1 + blk.b[p][2][2] * i2;
         q += i0 * o0 + i1 * o1 + i2 * o2;
     }
-    dk[e] = -q;
+    if (ADJ)
+        dk[e] = adj.scale * simp_grad(adj.rho[e], adj.P) * (-q);
+    else
+        dk[e] = -q;
 }
 
-__global__ void k_sens_q4(int NX, int NY, const double* __restrict__ U, const Q4K<double> K, double* __restrict__ dk) {
+template <bool ADJ>
+__global__ void k_sens_q4(int NX, int NY, const double* __restrict__ U, const Q4K<double> K, AdjArgs adj,
+                          double* __restrict__ dk) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)NX * NY) return;
     const int i = (int)(e / NY), j = (int)(e % NY), nx = NX + 1;
@@ -575,19 +603,38 @@ __global__ void k_sens_q4(int NX, int NY, const double* __restrict__ U, const Q4
         for (int b = 0; b < 8; b++) s += K.k[a][b] * ue[b];
         out -= s * ue[a];
     }
-    dk[e] = out;
+    if (ADJ)
+        dk[e] = adj.scale * simp_grad(adj.rho[e], adj.P) * out;
+    else
+        dk[e] = out;
 }
 
-int launch_sensitivity(const Op* op, const double* U, double* dk, cudaStream_t st) {
+template <bool ADJ>
+static int launch_sens(const Op* op, const double* U, const AdjArgs& adj, double* out, cudaStream_t st) {
     const Grid& g = op->grid;
     const unsigned nb = (unsigned)((g.n_elem + 255) / 256);
     pf::count_launch();
     if (g.dim == 3)
-        k_sens_h8<<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], U, make_blk<double>(op), dk);
+        k_sens_h8<ADJ><<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], U, make_blk<double>(op), adj, out);
     else
-        k_sens_q4<<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], U, make_q4k<double>(op), dk);
+        k_sens_q4<ADJ><<<nb, 256, 0, st>>>(g.nel[0], g.nel[1], U, make_q4k<double>(op), adj, out);
     PF_LAUNCH_CHECK("sensitivity launch");
     return PF_OK;
+}
+
+int launch_sensitivity(const Op* op, const double* U, double* dk, cudaStream_t st) {
+    AdjArgs none;
+    memset(&none, 0, sizeof(none));
+    return launch_sens<false>(op, U, none, dk, st);
+}
+
+int launch_adjoint(const Op* op, const double* U, const double* rho, const pf_simp_params& P, double scale,
+                   double* out, cudaStream_t st) {
+    AdjArgs a;
+    a.rho = rho;
+    a.P = P;
+    a.scale = scale;
+    return launch_sens<true>(op, U, a, out, st);
 }
 
 __global__ void k_pack_mask(long long n_nodes, int dof, const uint8_t* __restrict__ con, uint8_t* __restrict__ mask) {

@@ -29,6 +29,8 @@ long long fine_matvec_num_blocks(const Op* op, int fp32);
 template <typename T>
 int launch_diagonal(const Op* op, const double* E, const uint8_t* mask, T* diag, cudaStream_t st);
 int launch_sensitivity(const Op* op, const double* U, double* dk, cudaStream_t st);
+int launch_adjoint(const Op* op, const double* U, const double* rho, const pf_simp_params& P, double scale,
+                   double* out, cudaStream_t st);
 int launch_pack_mask(const Op* op, const uint8_t* con, uint8_t* mask, cudaStream_t st);
 
 }  // namespace pf
