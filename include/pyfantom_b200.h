@@ -190,6 +190,56 @@ size_t pf_oc_workspace_size(long long n); /* doubles */
 int pf_oc_update_f64(long long n, const double* x, const double* df, const double* dg, double vf,
                      double move, double* x_new, double* work, double* h_out, void* stream);
 
+/* ---- learned warm start: kernels of a small 3D convolutional network ---------------
+ * No counterpart in the reference (the learned form of this library).  float32
+ * activations [N][C][X][Y][Z], weights [Cout][Cin][3][3][3], zero padding 1, stride 1|2
+ * (output extent (n-1)/stride + 1).  relu != 0 fuses max(0, .) into the forward. */
+int pf_cnn_conv3d_fwd_f32(const float* x, int N, int Cin, int X, int Y, int Z, const float* w, const float* b,
+                          int Cout, int stride, int relu, float* y, void* stream);
+/* dx = W^T dy (accumulate != 0: dx += W^T dy) */
+int pf_cnn_conv3d_bwd_data_f32(const float* dy, int N, int Cin, int X, int Y, int Z, const float* w, int Cout,
+                               int stride, int accumulate, float* dx, void* stream);
+size_t pf_cnn_conv3d_bwd_weight_workspace(int Cin, int Cout); /* floats */
+int pf_cnn_conv3d_bwd_weight_f32(const float* x, const float* dy, int N, int Cin, int X, int Y, int Z, int Cout,
+                                 int stride, float* dw, float* db, float* work, void* stream);
+int pf_cnn_relu_bwd_f32(long long n, const float* y, float* dy, void* stream); /* dy *= (y > 0) */
+/* nearest 2x upsampling of NC channels of X x Y x Z (backward: x = dy fine, y = dx coarse) */
+int pf_cnn_upsample2_f32(int NC, int X, int Y, int Z, const float* x, float* y, int backward, void* stream);
+/* dst[n][c_off + c] (+)= src[n][c] for c < Csrc; gather != 0 copies the other way */
+int pf_cnn_copy_channels_f32(int N, int Csrc, long long V, const float* src, int Cdst, int c_off, int accumulate,
+                             int gather, float* dst, void* stream);
+/* out[n][c] = scale * sum_v src[n][c_off + c][v] (src has Csrc channels of V voxels) */
+int pf_cnn_channel_sum_f32(int N, int C, long long V, const float* src, int Csrc, int c_off, float scale, float* out,
+                           void* stream);
+/* dst[n][c_off + c][v] (+)= scale * g[n][c] for every voxel v (dst has Cdst channels) */
+int pf_cnn_channel_bcast_f32(int N, int C, long long V, const float* g, float scale, int Cdst, int c_off,
+                             int accumulate, float* dst, void* stream);
+/* cells [N][3][X][Y][Z] -> nodal 3-vectors [N][nodes][3] (mean of adjacent cells), or back */
+int pf_cnn_cell2node_f32(int N, int X, int Y, int Z, const float* in, float* out, int backward, void* stream);
+size_t pf_cnn_mse_workspace(long long n); /* doubles */
+/* loss = mean((pred - target)^2) into the device double *loss; grad (may be NULL) = d loss / d pred */
+int pf_cnn_mse_f32(long long n, const float* pred, const float* target, float* grad, double* loss, double* work,
+                   void* stream);
+/* one bias-corrected Adam step (step counts from 1) */
+int pf_cnn_adam_f32(long long n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2,
+                    float eps, int step, void* stream);
+/* Network input of one sample on the cell grid fine->nel / P (every count divisible by P):
+ * out [8][X/P][Y/P][Z/P] = E^(1/3) of the block-mean stiffness; nodal forces of the
+ * block's closed node box (shared nodes split between blocks) divided by max|f|; the
+ * constrained fraction of the 24 DOFs at the cell corners; cell-centre coordinates
+ * scaled to (-1, 1).  E [elements], f [dof] device doubles, node_mask from pf_pack_mask
+ * (NULL: unconstrained), work: 1 unsigned. */
+int pf_cnn_features_f32(const pf_grid* fine, int P, const double* E, const double* f, const uint8_t* node_mask,
+                        unsigned* work, float* out, void* stream);
+/* x0 [dof] = trilinear interpolation onto the fine mesh of the nodal field coarse_nodes
+ * [(X/P+1)(Y/P+1)(Z/P+1)][3] of the mesh with nel / P elements; 0 on constrained DOFs. */
+int pf_cnn_guess_f64(const pf_grid* fine, int P, const float* coarse_nodes, const uint8_t* node_mask, double* x0,
+                     void* stream);
+/* x0 *= alpha = (x0.b) / (x0.Kx0) (0 if x0.Kx0 <= 0); work: pf_cnn_energy_scale_workspace()
+ * doubles; work[size - 2] = alpha, work[size - 1] = ||b - alpha Kx0|| / ||b||. */
+size_t pf_cnn_energy_scale_workspace(void);
+int pf_cnn_energy_scale_f64(long long n, double* x0, const double* Kx0, const double* b, double* work, void* stream);
+
 /* ---- OC update without allocation --------------------------------------------------
  * No counterpart in the reference.  Same computation and outputs as pf_oc_update_f64,
  * for callers that cannot allocate device memory where they run the OC step (code being

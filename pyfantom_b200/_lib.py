@@ -97,6 +97,24 @@ SIGNATURES = {
     "pf_oc_workspace_size": (_SZ, [_LL]),
     "pf_oc_update_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
     "pf_oc_update_noalloc_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "pf_cnn_conv3d_fwd_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P]),
+    "pf_cnn_conv3d_bwd_data_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P]),
+    "pf_cnn_conv3d_bwd_weight_workspace": (_SZ, [_I, _I]),
+    "pf_cnn_conv3d_bwd_weight_f32": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P]),
+    "pf_cnn_relu_bwd_f32": (_I, [_LL, _P, _P, _P]),
+    "pf_cnn_upsample2_f32": (_I, [_I, _I, _I, _I, _P, _P, _I, _P]),
+    "pf_cnn_copy_channels_f32": (_I, [_I, _I, _LL, _P, _I, _I, _I, _I, _P, _P]),
+    "pf_cnn_channel_sum_f32": (_I, [_I, _I, _LL, _P, _I, _I, ctypes.c_float, _P, _P]),
+    "pf_cnn_channel_bcast_f32": (_I, [_I, _I, _LL, _P, ctypes.c_float, _I, _I, _I, _P, _P]),
+    "pf_cnn_cell2node_f32": (_I, [_I, _I, _I, _I, _P, _P, _I, _P]),
+    "pf_cnn_mse_workspace": (_SZ, [_LL]),
+    "pf_cnn_mse_f32": (_I, [_LL, _P, _P, _P, _P, _P, _P]),
+    "pf_cnn_adam_f32": (_I, [_LL, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                             _I, _P]),
+    "pf_cnn_features_f32": (_I, [ctypes.POINTER(pf_grid), _I, _P, _P, _P, _P, _P, _P]),
+    "pf_cnn_guess_f64": (_I, [ctypes.POINTER(pf_grid), _I, _P, _P, _P, _P]),
+    "pf_cnn_energy_scale_workspace": (_SZ, []),
+    "pf_cnn_energy_scale_f64": (_I, [_LL, _P, _P, _P, _P, _P]),
 }
 
 _lib = None
