@@ -6,7 +6,9 @@
   hierarchy and normalised transfers; the coarse solve is a dense Cholesky on the
   device instead of host CHOLMOD (every reference ``coarse_solver`` name maps to it,
   with the same ``beta = 1e-6`` shift).  Keyword-only extras: ``precision`` ('fp64' or
-  'mixed': FP32 V-cycle inside the FP64 CG) and ``check_every`` (host poll interval).
+  'mixed': FP32 V-cycle inside the FP64 CG), ``check_every`` (host poll interval) and
+  ``warm_start`` (an object with ``guess(kernel, rhs)``, e.g. learned.LearnedWarmStart,
+  that supplies the initial guess of a solve that does not reuse ``last_x0``).
 
 ``solve(rhs, rho=None, use_last=True)`` returns ``(U, residual)`` like the reference;
 ``last_x0`` holds the warm start.  Solver statistics of the last call are in
@@ -96,8 +98,10 @@ class MultiGrid(Solver):
 
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="cholmod", matrix_free=False, low_level_tol=1e-8,
-                 low_level_maxiter=5000, min_omega=0.4, omega_boost=1.06, *, precision="fp64", check_every=4):
+                 low_level_maxiter=5000, min_omega=0.4, omega_boost=1.06, *, precision="fp64", check_every=4,
+                 warm_start=None):
         self.kernel = kernel
+        self.warm_start = warm_start
         self.mesh = mesh
         self.last_x0 = None
         self.tol = tol
@@ -185,7 +189,13 @@ class MultiGrid(Solver):
         rhs = as_cuda(rhs, torch.float64)
         n = rhs.shape[0]
         warm = use_last and self.last_x0 is not None
-        x = self.last_x0 if warm else torch.empty(n, dtype=torch.float64, device=device())
+        if warm:
+            x = self.last_x0
+        elif self.warm_start is not None:
+            x = self.warm_start.guess(k, rhs).clone()
+            warm = True
+        else:
+            x = torch.empty(n, dtype=torch.float64, device=device())
         self.setup()
         info = _lib.pf_solve_info()
         _lib.check(_lib.load().pf_mg_solve(self._mg, _lib.ptr(rhs), _lib.ptr(x), int(warm), float(self.tol),
