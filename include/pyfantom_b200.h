@@ -240,6 +240,14 @@ int pf_cnn_guess_f64(const pf_grid* fine, int P, const float* coarse_nodes, cons
 size_t pf_cnn_energy_scale_workspace(void);
 int pf_cnn_energy_scale_f64(long long n, double* x0, const double* Kx0, const double* b, double* work, void* stream);
 
+/* Energy-deficit training loss of a nodal prediction y for K u = b (y zero on constrained
+ * DOFs, Ky = K y, c = b.u > 0): loss = 1 - (b.y)^2 / ((y.Ky) c), the relative energy
+ * error left after scaling y by (b.y)/(y.Ky); grad [n] float = d loss / d y.
+ * work: pf_cnn_energy_loss_workspace() doubles. */
+size_t pf_cnn_energy_loss_workspace(void);
+int pf_cnn_energy_loss_f64(long long n, const double* y, const double* Ky, const double* b, double c, float* grad,
+                           double* loss, double* work, void* stream);
+
 /* ---- OC update without allocation --------------------------------------------------
  * No counterpart in the reference.  Same computation and outputs as pf_oc_update_f64,
  * for callers that cannot allocate device memory where they run the OC step (code being

@@ -115,6 +115,8 @@ SIGNATURES = {
     "pf_cnn_guess_f64": (_I, [ctypes.POINTER(pf_grid), _I, _P, _P, _P, _P]),
     "pf_cnn_energy_scale_workspace": (_SZ, []),
     "pf_cnn_energy_scale_f64": (_I, [_LL, _P, _P, _P, _P, _P]),
+    "pf_cnn_energy_loss_workspace": (_SZ, []),
+    "pf_cnn_energy_loss_f64": (_I, [_LL, _P, _P, _P, _D, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -505,6 +505,41 @@ __global__ void k_scale_apply(long long n, const double* __restrict__ part, doub
         x[i] *= alpha;
 }
 
+// Energy deficit of the best multiple of y (the Rayleigh-Ritz principle for K u = b):
+//   L = 1 - (b.y)^2 / ((y.Ky) c),  c = b.u the compliance of the exact solution,
+//   dL/dy = -2 (b.y) / ((y.Ky) c) (b - (b.y) / (y.Ky) Ky)
+// which is 1 - cos^2 of the angle between y and u in the energy inner product: the
+// energy error left after the guess is scaled by alpha = (y.b) / (y.Ky).
+__global__ void __launch_bounds__(256) k_energy_partials(long long n, const double* __restrict__ y,
+                                                         const double* __restrict__ ky, const double* __restrict__ b,
+                                                         double* __restrict__ part) {
+    __shared__ double red[8];
+    double sa = 0.0, sq = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        sa += b[i] * y[i];
+        sq += y[i] * ky[i];
+    }
+    sa = block_sum<256>(sa, red);
+    sq = block_sum<256>(sq, red);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = sa;
+        part[kScaleBlocks + blockIdx.x] = sq;
+    }
+}
+__global__ void k_energy_grad(long long n, const double* __restrict__ part, const double* __restrict__ ky,
+                              const double* __restrict__ b, double c, float* __restrict__ grad, double* __restrict__ loss) {
+    double a = 0.0, q = 0.0;
+    for (int i = 0; i < kScaleBlocks; i++) {
+        a += part[i];
+        q += part[kScaleBlocks + i];
+    }
+    const bool ok = q > 0.0 && c > 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *loss = ok ? 1.0 - a * a / (q * c) : 1.0;
+    const double s = ok ? -2.0 * a / (q * c) : 0.0, r = ok ? a / q : 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        grad[i] = (float)(s * (b[i] - r * ky[i]));
+}
+
 static unsigned gs(long long n) {
     long long b = (n + 255) / 256;
     if (b > 16LL * kNumSM) b = 16LL * kNumSM;
@@ -704,5 +739,18 @@ extern "C" int pf_cnn_energy_scale_f64(long long n, double* x0, const double* Kx
     k_scale_partials<<<kScaleBlocks, 256, 0, st>>>(n, x0, Kx0, b, work);
     k_scale_apply<<<gs(n), 256, 0, st>>>(n, work, x0, work + 5 * kScaleBlocks);
     PF_LAUNCH_CHECK("energy scale launch");
+    return PF_OK;
+}
+
+extern "C" size_t pf_cnn_energy_loss_workspace(void) { return 2 * kScaleBlocks; }
+
+extern "C" int pf_cnn_energy_loss_f64(long long n, const double* y, const double* Ky, const double* b, double c,
+                                      float* grad, double* loss, double* work, void* stream) {
+    if (n < 1 || !y || !Ky || !b || !grad || !loss || !work) return fail(PF_BAD_ARG, "pf_cnn_energy_loss_f64: bad argument");
+    cudaStream_t st = as_stream(stream);
+    count_launch(2);
+    k_energy_partials<<<kScaleBlocks, 256, 0, st>>>(n, y, Ky, b, work);
+    k_energy_grad<<<gs(n), 256, 0, st>>>(n, work, Ky, b, c, grad, loss);
+    PF_LAUNCH_CHECK("energy loss launch");
     return PF_OK;
 }

@@ -23,11 +23,14 @@ load, the Dirichlet fraction and the cell-centre coordinates; the coordinates an
 global context g let the field at one end of the mesh depend on a load at the other,
 beyond the roughly 40-cell receptive field of the convolutions.
 
-Cell outputs become nodal displacements by averaging the adjacent cells.  The training
-loss is the mean-squared error against solver displacements normalised to unit RMS per
-sample (the scale is recovered by alpha at use).  Forward, backward (input and weight
-gradients), the loss and the Adam update are the ``pf_cnn_*`` kernels; torch only holds
-the buffers.  This form has no counterpart in the reference.
+Cell outputs become nodal displacements by averaging the adjacent cells.  Two training
+losses are available.  ``energy`` (the default) is what the CG pays for: the relative
+energy error left after the energy-optimal scaling, 1 - (b.y)^2 / ((y.Ky) b.u) by the
+Rayleigh-Ritz principle, evaluated with one stiffness matvec per sample
+(``pf_cnn_energy_loss_f64``).  ``mse`` is the mean-squared error against solver
+displacements normalised to unit RMS per sample.  Forward, backward (input and weight
+gradients), the losses and the Adam update are the ``pf_cnn_*`` kernels; torch only
+holds the buffers.  This form has no counterpart in the reference.
 """
 from __future__ import annotations
 
@@ -42,8 +45,8 @@ import torch
 from . import _lib
 from ._tensor import as_cuda, device
 
-__all__ = ["WarmStartNet", "LearnedWarmStart", "make_dataset", "random_edge_load", "cantilever_constraints",
-           "DEFAULT_WEIGHTS"]
+__all__ = ["WarmStartNet", "LearnedWarmStart", "EnergyLoss", "make_dataset", "random_edge_load",
+           "cantilever_constraints", "edge_load_rhs", "DEFAULT_WEIGHTS"]
 
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_unet_64x32x32.npz")
 N_IN = 8
@@ -307,29 +310,61 @@ class WarmStartNet:
                                         _lib.stream()))
         return float(losses.mean())
 
+    def energy_loss_and_grad(self, x, idx, energy, loss_out):
+        """Forward, the energy-deficit loss of each sample (``energy``: an EnergyLoss over
+        the data set, ``idx``: the samples' indices in it) into ``loss_out`` [N], and
+        backward."""
+        nodes = self.predict_nodes(x)
+        N, _, X, Y, Z = x.shape
+        b = self._buffers(N, X, Y, Z)
+        for s, i in enumerate(idx):
+            energy.sample(int(i), nodes[s], b["g_nodes"][s], loss_out[s:s + 1])
+        _lib.check(_lib.load().pf_cnn_cell2node_f32(N, X, Y, Z, _p(b["g_nodes"]), _p(b["g_out"]), 1, _lib.stream()))
+        return self.backward(b["g_out"])
+
+    def eval_energy(self, inputs, energy, batch=8):
+        """Mean energy deficit over a data set (forward only)."""
+        S = inputs.shape[0]
+        losses = torch.zeros(S, dtype=torch.float64, device=inputs.device)
+        for it in range(S // batch):
+            xb = inputs[it * batch:(it + 1) * batch]
+            nodes = self.predict_nodes(xb)
+            b = self._buffers(*xb.shape[:1], *xb.shape[2:])
+            for s in range(batch):
+                k = it * batch + s
+                energy.sample(k, nodes[s], b["g_nodes"][s], losses[k:k + 1])
+        return float(losses[:(S // batch) * batch].mean())
+
     # ---- training -------------------------------------------------------------------
-    def fit(self, inputs, targets, epochs=20, batch=8, lr=1e-3, lr_final=1e-4, seed=0, log=None):
-        """Adam on the node MSE over ``inputs`` [S, 8, X, Y, Z] / ``targets`` [S, nodes * 3]
-        (device float32), cosine learning-rate decay from lr to lr_final.  Returns the mean
-        loss of every epoch."""
+    def fit(self, inputs, targets, epochs=20, batch=8, lr=1e-3, lr_final=1e-4, seed=0, log=None, energy=None):
+        """Adam over ``inputs`` [S, 8, X, Y, Z] (device float32) on the node MSE against
+        ``targets`` [S, nodes * 3], or on the energy deficit when ``energy`` (an EnergyLoss
+        over the same samples) is given; cosine learning-rate decay from lr to lr_final.
+        Returns the mean loss of every epoch."""
         S = inputs.shape[0]
         steps = S // batch
         gen = torch.Generator().manual_seed(seed)
-        losses = torch.zeros(epochs * steps, dtype=torch.float64, device=inputs.device)
+        per = batch if energy is not None else 1
+        losses = torch.zeros(epochs * steps * per, dtype=torch.float64, device=inputs.device)
         hist = []
         total = epochs * steps
         for ep in range(epochs):
-            perm = torch.randperm(S, generator=gen).to(inputs.device)
+            perm_h = torch.randperm(S, generator=gen)
+            perm = perm_h.to(inputs.device)
             t0 = time.time()
             for it in range(steps):
                 k = ep * steps + it
                 idx = perm[it * batch:(it + 1) * batch]
                 xb = inputs.index_select(0, idx)
-                yb = targets.index_select(0, idx)
-                self.loss_and_grad(xb, yb, losses[k:k + 1])
+                if energy is not None:
+                    self.energy_loss_and_grad(xb, perm_h[it * batch:(it + 1) * batch].tolist(), energy,
+                                              losses[k * per:(k + 1) * per])
+                else:
+                    yb = targets.index_select(0, idx)
+                    self.loss_and_grad(xb, yb, losses[k:k + 1])
                 lr_k = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * k / total))
                 self.adam(lr=lr_k)
-            hist.append(float(losses[ep * steps:(ep + 1) * steps].mean()))
+            hist.append(float(losses[ep * steps * per:(ep + 1) * steps * per].mean()))
             if log is not None:
                 log(f"epoch {ep + 1}/{epochs} loss {hist[-1]:.5f} ({time.time() - t0:.1f} s)")
         return hist
@@ -372,10 +407,36 @@ def edge_load_rhs(nel, seed):
     return f
 
 
-def make_dataset(n_samples, nel=(64, 32, 32), seed0=1000, n_level=4, tol=1e-8, log=None):
+class EnergyLoss:
+    """Per-sample energy-deficit loss over a data set of cantilever problems sharing one
+    mesh and constraint set (``kern``): E [S, elements] and f [S, dof] device doubles,
+    compliances c [S] (host floats)."""
+
+    def __init__(self, kern, E, f, c):
+        self.kern, self.E, self.f, self.c = kern, E, f, [float(v) for v in c]
+        n = f.shape[1]
+        dev = f.device
+        self.y = torch.empty(n, dtype=torch.float64, device=dev)
+        self.ky = torch.empty(n, dtype=torch.float64, device=dev)
+        self.work = torch.empty(int(_lib.load().pf_cnn_energy_loss_workspace()), dtype=torch.float64, device=dev)
+
+    def sample(self, i, nodes, grad, loss_out):
+        """loss_out = deficit of the nodal prediction ``nodes`` (float32) for sample i;
+        grad (float32, nodes' layout) = its gradient."""
+        L = _lib.load()
+        k = self.kern
+        Ei, fi = self.E[i], self.f[i]
+        _lib.check(L.pf_cnn_guess_f64(ctypes.byref(k._grid), 1, _p(nodes), k._mask_ptr(), _p(self.y), _lib.stream()))
+        _lib.check(L.pf_matvec_f64(k._op, _p(Ei), _p(self.y), k._mask_ptr(), _p(self.ky), _lib.stream()))
+        _lib.check(L.pf_cnn_energy_loss_f64(self.y.numel(), _p(self.y), _p(self.ky), _p(fi), self.c[i], _p(grad),
+                                            _p(loss_out), _p(self.work), _lib.stream()))
+
+
+def make_dataset(n_samples, nel=(64, 32, 32), seed0=1000, n_level=4, tol=1e-8, log=None, keep_problems=False):
     """(inputs [S, 8, X, Y, Z], targets [S, nodes * 3], solve statistics) from cold-start
     FP64 MGCG solves of cantilevers clamped at x = 0 with seeded smoothed-random densities
-    (sigma 2, SIMP p = 3) and a random edge load (sample i uses seed seed0 + i)."""
+    (sigma 2, SIMP p = 3) and a random edge load (sample i uses seed seed0 + i).  With
+    ``keep_problems`` the statistics also hold ``energy``, an EnergyLoss over the samples."""
     from .geom import CuStructuredMesh3D
     from .physics import LinearElasticity
     from .solvers import MultiGrid
@@ -392,7 +453,10 @@ def make_dataset(n_samples, nel=(64, 32, 32), seed0=1000, n_level=4, tol=1e-8, l
     targets = torch.empty((n_samples, D), dtype=torch.float32, device=device())
     g = _lib.make_grid(nel)
     work = torch.zeros(1, dtype=torch.int32, device=device())
-    its, res = [], []
+    its, res, comp = [], [], []
+    if keep_problems:
+        Es = torch.empty((n_samples, nelx * nely * nelz), dtype=torch.float64, device=device())
+        fs = torch.empty((n_samples, D), dtype=torch.float64, device=device())
     t0 = time.time()
     for s in range(n_samples):
         E = as_cuda(simp_E(smoothed_density(nel, seed0 + s)), torch.float64)
@@ -402,12 +466,19 @@ def make_dataset(n_samples, nel=(64, 32, 32), seed0=1000, n_level=4, tol=1e-8, l
             raise RuntimeError(f"training solve {seed0 + s} ended with {sol.last_info['status']} at residual {r:.3e}")
         its.append(sol.last_info["iterations"])
         res.append(r)
+        comp.append(float(torch.dot(f, U)))
+        if keep_problems:
+            Es[s].copy_(E)
+            fs[s].copy_(f)
         _lib.check(_lib.load().pf_cnn_features_f32(ctypes.byref(g), 1, _p(E), _p(f), kern._mask_ptr(), _p(work),
                                                    _p(inputs[s]), _lib.stream()))
         targets[s].copy_(U / U.square().mean().sqrt())
         if log is not None and (s + 1) % 250 == 0:
             log(f"dataset {s + 1}/{n_samples} ({time.time() - t0:.1f} s, mean iterations {np.mean(its):.1f})")
-    return inputs, targets, dict(iterations=its, residuals=res, seconds=time.time() - t0)
+    stats = dict(iterations=its, residuals=res, compliances=comp, seconds=time.time() - t0)
+    if keep_problems:
+        stats["energy"] = EnergyLoss(kern, Es, fs, comp)
+    return inputs, targets, stats
 
 
 class LearnedWarmStart:
@@ -452,6 +523,7 @@ class LearnedWarmStart:
                                       _lib.stream()))
         _lib.check(L.pf_matvec_f64(kern._op, _p(kern.rho), _p(b["x0"]), kern._mask_ptr(), _p(b["kx"]), _lib.stream()))
         _lib.check(L.pf_cnn_energy_scale_f64(n, _p(b["x0"]), _p(b["kx"]), _p(rhs), _p(b["scale"]), _lib.stream()))
+        self.x0 = b["x0"]
         if self.read_stats:
             a, r = b["scale"][-2:].tolist()
             self.last = dict(alpha=a, residual=r)

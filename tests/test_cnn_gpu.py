@@ -193,6 +193,26 @@ def test_features_guess_and_scale(pool):
     assert abs(float(sw[-1]) - np.linalg.norm(b - alpha * kx) / np.linalg.norm(b)) < 1e-12
 
 
+def test_energy_loss_kernel():
+    rng = np.random.default_rng(9)
+    n = 5000
+    A = rng.normal(size=(50, n)) / 10
+    y, u = rng.normal(size=n), rng.normal(size=n)
+    # K = A^T A + I restricted to a random subspace is SPD; only Ky and b = Ku enter
+    ky = A.T @ (A @ y) + y
+    b = A.T @ (A @ u) + u
+    c = float(b @ u)
+    yt, kyt, bt = (torch.as_tensor(v, device="cuda") for v in (y, ky, b))
+    grad = torch.empty(n, dtype=torch.float32, device="cuda")
+    loss = torch.empty(1, dtype=torch.float64, device="cuda")
+    work = torch.empty(int(lib().pf_cnn_energy_loss_workspace()), dtype=torch.float64, device="cuda")
+    _lib.check(lib().pf_cnn_energy_loss_f64(n, P(yt), P(kyt), P(bt), c, P(grad), P(loss), P(work), S()))
+    a, q = b @ y, y @ ky
+    assert abs(float(loss) - (1 - a * a / (q * c))) < 1e-12
+    assert relerr(grad, -2 * a / (q * c) * (b - a / q * ky)) < 1e-6
+    assert 0.0 <= float(loss) <= 1.0
+
+
 def test_network_gradient_matches_oracle():
     net = learned.WarmStartNet(channels=(4, 4, 8, 8), seed=3)
     rng = np.random.default_rng(4)
@@ -229,6 +249,13 @@ def test_training_reduces_loss():
     net = learned.WarmStartNet(channels=(8, 8, 16, 16), seed=0)
     hist = net.fit(inputs, targets, epochs=25, batch=4, lr=2e-3, lr_final=2e-4, seed=0)
     assert hist[-1] < 0.75 * hist[0], hist
+    # the energy deficit (1 - cos^2 in the energy inner product) falls as well
+    inputs, targets, stats = learned.make_dataset(48, nel=(16, 8, 8), seed0=1000, n_level=2, keep_problems=True)
+    net = learned.WarmStartNet(channels=(8, 8, 16, 16), seed=0)
+    d0 = net.eval_energy(inputs, stats["energy"], batch=4)
+    hist = net.fit(inputs, targets, epochs=25, batch=4, lr=2e-3, lr_final=2e-4, seed=0, energy=stats["energy"])
+    d1 = net.eval_energy(inputs, stats["energy"], batch=4)
+    assert 0.0 <= d1 < 0.5 * d0 <= 0.5, (d0, d1, hist)
 
 
 def _held_out(nel, seed, n_level, ws, precision="fp64"):
