@@ -105,7 +105,7 @@ class Clocks:
 # -----------------------------------------------------------------------------------------
 # our arm
 # -----------------------------------------------------------------------------------------
-def build_problem(nel, n_level, precision="fp64", tol=1e-8):
+def build_problem(nel, n_level, precision="fp64", tol=1e-8, warm_start=None):
     import torch
     from pyfantom_b200 import workloads
     from pyfantom_b200.CUDA import FiniteElement, MultiGrid, StructuredMesh3D, StructuredStiffnessKernel
@@ -113,7 +113,8 @@ def build_problem(nel, n_level, precision="fp64", tol=1e-8):
     wl = workloads.cantilever3d(*nel)
     mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
     kern = StructuredStiffnessKernel(mesh)
-    sol = MultiGrid(mesh, kern, maxiter=1000, tol=tol, n_smooth=2, omega=0.6, n_level=n_level, precision=precision)
+    sol = MultiGrid(mesh, kern, maxiter=1000, tol=tol, n_smooth=2, omega=0.6, n_level=n_level, precision=precision,
+                    warm_start=warm_start)
     fe = FiniteElement(mesh, kern, sol)
     fe.add_dirichlet_boundary_condition(node_ids=torch.as_tensor(wl["fixed_nodes"], device="cuda"), rhs=0.0)
     fe.add_point_forces(forces=wl["load_forces"], node_ids=torch.as_tensor(wl["load_nodes"], device="cuda"))
@@ -238,9 +239,55 @@ def run_ours(args, rank, world, local_rank):
     return result, (wl, mesh)
 
 
+def forms_256():
+    """The three solver forms at the 256x128x128 cantilever (12.8M DOF, 5 levels, tol 1e-8,
+    cold start): plain FP64 MGCG, mixed precision (FP32 V-cycle in FP64 CG) and mixed
+    precision from the learned guess (network on the 64x32x32 pooled cell grid, trilinear
+    interpolation, energy-optimal scale; its inference is inside the timed solve).  Each
+    form: median of 3 timed solves after 1 warm-up, L2 flushed before each."""
+    import torch
+    from pyfantom_b200 import learned
+    nel, nl = (256, 128, 128), 5
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out, ref = {}, None
+    ws = learned.LearnedWarmStart(learned.WarmStartNet.load(), pool=4, read_stats=False)
+    for name, prec, w in (("fp64", "fp64", None), ("mixed", "mixed", None), ("mixed_learned", "mixed", ws)):
+        wl, mesh, kern, sol, fe, E = build_problem(nel, nl, prec, warm_start=w)
+        kern.set_rho(E)
+        U, _ = sol.solve(fe.rhs, use_last=False)
+        t = []
+        for _ in range(3):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            kern.set_rho(E)
+            U, _ = sol.solve(fe.rhs, use_last=False)
+            e1.record()
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1))
+        r = fe.rhs - kern.dot(U)
+        c = float(torch.dot(fe.rhs, U))
+        ms = statistics.median(t)
+        out[name] = {"solves_per_s": round(1e3 / ms, 3), "ms": round(ms, 2),
+                     "pcg_iterations": sol.last_info["iterations"],
+                     "true_rel_residual": float(torch.linalg.norm(r) / torch.linalg.norm(fe.rhs)),
+                     "compliance": c}
+        if ref is None:
+            ref = (c, U.clone())
+        else:
+            out[name]["rel_compliance_err_vs_fp64"] = abs(c - ref[0]) / abs(ref[0])
+            out[name]["rel_displacement_err_vs_fp64"] = float(torch.linalg.norm(U - ref[1]) / torch.linalg.norm(ref[1]))
+            out[name]["speedup_vs_fp64"] = round(out["fp64"]["ms"] / ms, 3)
+        del wl, mesh, kern, sol, fe, E, U, r
+    if ws.x0 is not None:
+        out["mixed_learned"]["guess"] = "network on 64x32x32 cells (pool 4), energy-scaled"
+    return out
+
+
 def extras(args):
-    """Secondary measurements on one GPU: mixed-precision form at the same workload, and the
-    fine matvec at 256x128x128 (HBM-resident) in FP64 and FP32."""
+    """Secondary measurements on one GPU: mixed-precision form at the same workload, the
+    fine matvec at 256x128x128 (HBM-resident) in FP64 and FP32, and the three solver forms
+    at 256x128x128."""
     import torch
     out = {}
     spec = WORKLOADS[args.workload]
@@ -297,6 +344,8 @@ def extras(args):
         out[f"matvec_256x128x128_{prec}"] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts,
                                              "GB_per_s": round(byts / ms / 1e6, 1),
                                              "dof_matvecs_per_s": round(D / ms * 1e3, 1)}
+    del kern, mesh, u, y, Et
+    out["forms_256x128x128"] = forms_256()
     return out
 
 

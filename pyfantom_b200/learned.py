@@ -494,6 +494,7 @@ class LearnedWarmStart:
         self.pool = int(pool)
         self.read_stats = read_stats
         self.last = None
+        self.x0 = None
         self._scratch = {}
 
     def _buf(self, n, kern):
