@@ -29,6 +29,21 @@ static const int kCX[8] = {0, 1, 1, 0, 0, 1, 1, 0};
 static const int kCY[8] = {0, 0, 1, 1, 0, 0, 1, 1};
 static const int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
 
+// The 33 distinct nonzeros of the eight symmetric 3x3 class blocks of an isotropic box
+// element: class p, row i, column j (upper triangle of each block's nonzero pattern).
+static const int kCoefP[33] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3, 3, 4,
+                               4, 4, 5, 5, 5, 5, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7};
+static const int kCoefI[33] = {0, 0, 0, 1, 1, 2, 1, 1, 2, 0, 0, 2, 0, 0, 1, 2, 0,
+                               0, 1, 0, 0, 2, 1, 1, 1, 2, 0, 0, 0, 0, 1, 1, 2};
+static const int kCoefJ[33] = {0, 1, 2, 1, 2, 2, 1, 2, 2, 0, 2, 2, 0, 1, 1, 2, 0,
+                               1, 1, 0, 2, 2, 1, 1, 2, 2, 0, 0, 1, 2, 1, 2, 2};
+
+static bool h8_coef_nonzero(int p, int i, int j) {
+    for (int q = 0; q < 33; q++)
+        if (kCoefP[q] == p && ((kCoefI[q] == i && kCoefJ[q] == j) || (kCoefI[q] == j && kCoefJ[q] == i))) return true;
+    return false;
+}
+
 static int walsh(int m, int l, int dim) {
     int pos[3] = {kCX[l], kCY[l], dim == 3 ? kCZ[l] : 0};
     int s = 1;
@@ -74,6 +89,32 @@ int op_factorise(Op* op) {
     if (!(off <= 1e-12 * bmax))
         return fail(PF_UNSUPPORTED,
                     "K0 is not invariant under the element's axis reflections (off-block %.3e vs %.3e)", off, bmax);
+    op->sparse = 0;
+    op->cube = 0;
+    if (dim == 3) {
+        // Isotropic box elements: each class block is symmetric and zero outside the
+        // pattern below (the rows of the rigid translations vanish, and reflection
+        // symmetry decouples the rest), leaving 33 distinct coefficients.
+        const double tol = 1e-12 * bmax;
+        bool ok = true;
+        for (int p = 0; p < 8; p++)
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    if (fabs(op->blk[p][i][j] - op->blk[p][j][i]) > tol) ok = false;
+                    if (!h8_coef_nonzero(p, i, j) && fabs(op->blk[p][i][j]) > tol) ok = false;
+                }
+        if (ok) {
+            for (int q = 0; q < 33; q++) op->coef[q] = op->blk[kCoefP[q]][kCoefI[q]][kCoefJ[q]];
+            op->sparse = 1;
+            // cube element: seven values in the pattern of cube_index()
+            const int rep[7] = {0, 1, 7, 12, 15, 27, 28};
+            for (int v = 0; v < 7; v++) op->cube_v[v] = op->coef[rep[v]];
+            bool cube = true;
+            for (int q = 0; q < 33; q++)
+                if (fabs(op->coef[q] - op->cube_v[cube_index(q)]) > tol) cube = false;
+            op->cube = cube ? 1 : 0;
+        }
+    }
     return PF_OK;
 }
 
@@ -84,6 +125,18 @@ template <typename T>
 struct H8Blk {
     T b[8][3][3];
 };
+template <typename T>
+struct H8Coef {
+    T c[33];  // sparse coefficients (CM 1) or the 7 cube values (CM 2)
+};
+// coefficient q of the sparse class blocks (CM 1: 33 values, CM 2: 7 cube values)
+template <int Q, int CM, typename T>
+__device__ __forceinline__ T coef(const H8Coef<T>& cf) {
+    if constexpr (CM == 2)
+        return cf.c[cube_index(Q)];
+    else
+        return cf.c[Q];
+}
 
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -103,10 +156,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   3. wait for this thread's copies, zero the constrained components it copied,
 //      __syncthreads (the only barrier of the step);
 //   4. owners finish their node of plane ie and apply the epilogue.
-template <typename T, typename TE, int TY>
+// CM selects the element operator: 0 dense class blocks read from shared memory (any K0
+// with the reflection symmetry), 1 the 33 nonzeros of an isotropic box element, 2 the 7
+// values of a cube element (1, 2: coefficients held in registers).
+template <typename T, typename TE, int TY, int CM>
 __global__ void __launch_bounds__((TY + 1) * 32)
     k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
-                const uint8_t* __restrict__ mask, const H8Blk<T> blk, Epi<T> epi) {
+                const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
     constexpr int NW = TY + 1;
     constexpr int NT = NW * 32;
     constexpr int PR = TY + 2, PC = 33, NPE = PR * PC;
@@ -182,7 +238,7 @@ __global__ void __launch_bounds__((TY + 1) * 32)
         for (int d = 0; d < 3; d++) cp_async(&s_ep[slot][d][tid], src + 3 * n + d, TB_);
     };
 
-    if (tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
+    if (CM == 0 && tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
     // the coefficients are re-read from shared memory at every use (volatile) rather than
     // held in 72 (FP32) / 144 (FP64) registers for the whole kernel
     const volatile T* vb = s_blk;
@@ -238,30 +294,97 @@ __global__ void __launch_bounds__((TY + 1) * 32)
         // reads and writes exactly the modes (c=0: py,pz), (c=1: py^1,pz), (c=2: py,pz^1),
         // so x stage, two 3x3 blocks and the inverse x stage complete per pair.
         T G[3][2][2];
-#pragma unroll
-        for (int pyz = 0; pyz < 4; pyz++) {
-            const int py = pyz & 1, pz = pyz >> 1;
-            const int p0 = 2 * py + 4 * pz, p1 = p0 + 1;
-            // x stage of the three (component, y-mode, z-mode) slots of this pair
-            const T h0 = e * ghi[0][py][pz], h1 = e * ghi[1][py ^ 1][pz], h2 = e * ghi[2][py][pz ^ 1];
-            const T a0 = fma(e, glo[0][py][pz], h0), b0 = fma(-e, glo[0][py][pz], h0);
-            const T a1 = fma(e, glo[1][py ^ 1][pz], h1), b1 = fma(-e, glo[1][py ^ 1][pz], h1);
-            const T a2 = fma(e, glo[2][py][pz ^ 1], h2), b2 = fma(-e, glo[2][py][pz ^ 1], h2);
-            // class p0 (px = 0): comp 0 in x-mode 1, comps 1, 2 in x-mode 0
-            const T o00 = fma(BK(p0, 0, 0), b0, fma(BK(p0, 0, 1), a1, BK(p0, 0, 2) * a2));
-            const T o01 = fma(BK(p0, 1, 0), b0, fma(BK(p0, 1, 1), a1, BK(p0, 1, 2) * a2));
-            const T o02 = fma(BK(p0, 2, 0), b0, fma(BK(p0, 2, 1), a1, BK(p0, 2, 2) * a2));
-            // class p1 (px = 1): comp 0 in x-mode 0, comps 1, 2 in x-mode 1
-            const T o10 = fma(BK(p1, 0, 0), a0, fma(BK(p1, 0, 1), b1, BK(p1, 0, 2) * b2));
-            const T o11 = fma(BK(p1, 1, 0), a0, fma(BK(p1, 1, 1), b1, BK(p1, 1, 2) * b2));
-            const T o12 = fma(BK(p1, 2, 0), a0, fma(BK(p1, 2, 1), b1, BK(p1, 2, 2) * b2));
-            // inverse x stage: (x-mode 0, x-mode 1) -> lower face w0 - w1, upper face w0 + w1
-            G[0][py][pz] = (o10 - o00) + carry[0][py][pz];
-            carry[0][py][pz] = o10 + o00;
-            G[1][py ^ 1][pz] = (o01 - o11) + carry[1][py ^ 1][pz];
-            carry[1][py ^ 1][pz] = o01 + o11;
-            G[2][py][pz ^ 1] = (o02 - o12) + carry[2][py][pz ^ 1];
-            carry[2][py][pz ^ 1] = o02 + o12;
+        if constexpr (CM == 0) {
+    #pragma unroll
+            for (int pyz = 0; pyz < 4; pyz++) {
+                const int py = pyz & 1, pz = pyz >> 1;
+                const int p0 = 2 * py + 4 * pz, p1 = p0 + 1;
+                // x stage of the three (component, y-mode, z-mode) slots of this pair
+                const T h0 = e * ghi[0][py][pz], h1 = e * ghi[1][py ^ 1][pz], h2 = e * ghi[2][py][pz ^ 1];
+                const T a0 = fma(e, glo[0][py][pz], h0), b0 = fma(-e, glo[0][py][pz], h0);
+                const T a1 = fma(e, glo[1][py ^ 1][pz], h1), b1 = fma(-e, glo[1][py ^ 1][pz], h1);
+                const T a2 = fma(e, glo[2][py][pz ^ 1], h2), b2 = fma(-e, glo[2][py][pz ^ 1], h2);
+                // class p0 (px = 0): comp 0 in x-mode 1, comps 1, 2 in x-mode 0
+                const T o00 = fma(BK(p0, 0, 0), b0, fma(BK(p0, 0, 1), a1, BK(p0, 0, 2) * a2));
+                const T o01 = fma(BK(p0, 1, 0), b0, fma(BK(p0, 1, 1), a1, BK(p0, 1, 2) * a2));
+                const T o02 = fma(BK(p0, 2, 0), b0, fma(BK(p0, 2, 1), a1, BK(p0, 2, 2) * a2));
+                // class p1 (px = 1): comp 0 in x-mode 0, comps 1, 2 in x-mode 1
+                const T o10 = fma(BK(p1, 0, 0), a0, fma(BK(p1, 0, 1), b1, BK(p1, 0, 2) * b2));
+                const T o11 = fma(BK(p1, 1, 0), a0, fma(BK(p1, 1, 1), b1, BK(p1, 1, 2) * b2));
+                const T o12 = fma(BK(p1, 2, 0), a0, fma(BK(p1, 2, 1), b1, BK(p1, 2, 2) * b2));
+                // inverse x stage: (x-mode 0, x-mode 1) -> lower face w0 - w1, upper face w0 + w1
+                G[0][py][pz] = (o10 - o00) + carry[0][py][pz];
+                carry[0][py][pz] = o10 + o00;
+                G[1][py ^ 1][pz] = (o01 - o11) + carry[1][py ^ 1][pz];
+                carry[1][py ^ 1][pz] = o01 + o11;
+                G[2][py][pz ^ 1] = (o02 - o12) + carry[2][py][pz ^ 1];
+                carry[2][py][pz ^ 1] = o02 + o12;
+            }
+        } else {
+#define KC(q) coef<q, CM, T>(cf)
+            // x stage of slot (component c, y-mode ym, z-mode zm): a = x-mode 0, b = x-mode 1
+#define XST(c, ym, zm, A, B)                          \
+    const T A = e * (ghi[c][ym][zm] + glo[c][ym][zm]); \
+    const T B = e * (ghi[c][ym][zm] - glo[c][ym][zm]);
+            // inverse x stage for pair (py, pz): classes p0 (outputs o0*) and p1 (o1*)
+#define XINV(py, pz, o00, o01, o02, o10, o11, o12)                  \
+    G[0][py][pz] = ((o10) - (o00)) + carry[0][py][pz];              \
+    carry[0][py][pz] = (o10) + (o00);                               \
+    G[1][(py) ^ 1][pz] = ((o01) - (o11)) + carry[1][(py) ^ 1][pz];  \
+    carry[1][(py) ^ 1][pz] = (o01) + (o11);                         \
+    G[2][py][(pz) ^ 1] = ((o02) - (o12)) + carry[2][py][(pz) ^ 1];  \
+    carry[2][py][(pz) ^ 1] = (o02) + (o12);
+            {  // pair (0,0): class 0 full, class 1 on components 1, 2
+                XST(0, 0, 0, a0, b0)
+                XST(1, 1, 0, a1, b1)
+                XST(2, 0, 1, a2, b2)
+                (void)a0;
+                const T o00 = fma(KC(0), b0, fma(KC(1), a1, KC(2) * a2));
+                const T o01 = fma(KC(1), b0, fma(KC(3), a1, KC(4) * a2));
+                const T o02 = fma(KC(2), b0, fma(KC(4), a1, KC(5) * a2));
+                const T o11 = fma(KC(6), b1, KC(7) * b2);
+                const T o12 = fma(KC(7), b1, KC(8) * b2);
+                XINV(0, 0, o00, o01, o02, T(0), o11, o12)
+            }
+            {  // pair (1,0): class 2 on components 0, 2; class 3 on 0, 1 and 2 alone
+                XST(0, 1, 0, a0, b0)
+                XST(1, 0, 0, a1, b1)
+                XST(2, 1, 1, a2, b2)
+                (void)a1;
+                const T o00 = fma(KC(9), b0, KC(10) * a2);
+                const T o02 = fma(KC(10), b0, KC(11) * a2);
+                const T o10 = fma(KC(12), a0, KC(13) * b1);
+                const T o11 = fma(KC(13), a0, KC(14) * b1);
+                const T o12 = KC(15) * b2;
+                XINV(1, 0, o00, T(0), o02, o10, o11, o12)
+            }
+            {  // pair (0,1): class 4 on components 0, 1; class 5 on 0, 2 and 1 alone
+                XST(0, 0, 1, a0, b0)
+                XST(1, 1, 1, a1, b1)
+                XST(2, 0, 0, a2, b2)
+                (void)a2;
+                const T o00 = fma(KC(16), b0, KC(17) * a1);
+                const T o01 = fma(KC(17), b0, KC(18) * a1);
+                const T o10 = fma(KC(19), a0, KC(20) * b2);
+                const T o11 = KC(22) * b1;
+                const T o12 = fma(KC(20), a0, KC(21) * b2);
+                XINV(0, 1, o00, o01, T(0), o10, o11, o12)
+            }
+            {  // pair (1,1): class 6 on 0 alone and 1, 2; class 7 full
+                XST(0, 1, 1, a0, b0)
+                XST(1, 0, 1, a1, b1)
+                XST(2, 1, 0, a2, b2)
+                const T o00 = KC(26) * b0;
+                const T o01 = fma(KC(23), a1, KC(24) * a2);
+                const T o02 = fma(KC(24), a1, KC(25) * a2);
+                const T o10 = fma(KC(27), a0, fma(KC(28), b1, KC(29) * b2));
+                const T o11 = fma(KC(28), a0, fma(KC(30), b1, KC(31) * b2));
+                const T o12 = fma(KC(29), a0, fma(KC(31), b1, KC(32) * b2));
+                XINV(1, 1, o00, o01, o02, o10, o11, o12)
+            }
+#undef XINV
+#undef XST
+#undef KC
         }
         // inverse z then y stage -> corner contributions t[c][b][cz]
         T t[3][2][2];
@@ -426,9 +549,25 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
         dim3 grid;
         int cx;
         h8_launch_dims(g, TY, &grid, &cx);
+        // FP32, isotropic box elements: the 33 nonzero coefficients (read as constant
+        // operands); FP64: the 7 values of a cube element in registers, other boxes the
+        // dense blocks from shared memory (33 double registers would cut the occupancy)
+        const int cm = sizeof(T) == 4 ? (op->sparse ? 1 : 0) : (op->cube ? 2 : 0);
+        H8Coef<T> cf;
+        for (int q = 0; q < 33; q++) cf.c[q] = T(0);
+        if (cm == 1)
+            for (int q = 0; q < 33; q++) cf.c[q] = (T)op->coef[q];
+        if (cm == 2)
+            for (int v = 0; v < 7; v++) cf.c[v] = (T)op->cube_v[v];
+        const H8Blk<T> blk = make_blk<T>(op);
         pf::count_launch();
-        k_matvec_h8<T, TE, TY><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
-                                                             make_blk<T>(op), epi);
+        constexpr int CMS = sizeof(T) == 4 ? 1 : 2;  // the sparse variant of this precision
+        if (cm != 0)
+            k_matvec_h8<T, TE, TY, CMS><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E,
+                                                                      mask, blk, cf, epi);
+        else
+            k_matvec_h8<T, TE, TY, 0><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
+                                                                    blk, cf, epi);
     } else {
         const long long nb = q4_num_blocks(g);
         pf::count_launch();

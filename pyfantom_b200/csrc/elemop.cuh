@@ -9,10 +9,26 @@ __host__ __device__ __forceinline__ int kCXd(int l) { return (0x66 >> l) & 1; }
 __host__ __device__ __forceinline__ int kCYd(int l) { return (0xCC >> l) & 1; }
 __host__ __device__ __forceinline__ int kCZd(int l) { return (0xF0 >> l) & 1; }
 
+// value index (0..6) of sparse coefficient q (see pf_op::coef) for a cube element:
+// class 0 a b b a b a | 1, 2 b c b | 3 d d d e | 4 b c b | 5, 6 d d d e | 7 f g g f g f
+__host__ __device__ constexpr int cube_index(int q) {
+    return q < 6 ? ((q == 0 || q == 3 || q == 5) ? 0 : 1)
+                 : q < 12 ? ((q - 6) % 3 == 1 ? 2 : 1)
+                 : q < 16 ? (q == 15 ? 4 : 3)
+                 : q < 19 ? (q == 17 ? 2 : 1)
+                 : q < 27 ? ((q == 22 || q == 26) ? 4 : 3)
+                 : ((q == 27 || q == 30 || q == 32) ? 5 : 6);
+}
+
 struct pf_op {
     pf::Grid grid;
     double K0[24 * 24];  // row-major element matrix (8x8 used in 2D)
     double blk[8][3][3]; // Walsh-class blocks of K0 (4 classes of 2x2 in 2D)
+    // 3D: the 33 distinct nonzeros of the class blocks when they have the sparsity of an
+    // isotropic box element (sparse != 0), and the 7 values of a cube element (cube != 0)
+    double coef[33];
+    int sparse, cube;
+    double cube_v[7];
 };
 
 namespace pf {

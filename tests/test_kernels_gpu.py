@@ -141,6 +141,45 @@ def test_matvec_anisotropic_element(lib):
     assert rel(op.matvec(E, u), O.matvec(nel, K0, E, u)) < 1e-12
 
 
+def _walsh_T():
+    cx, cy, cz = [0, 1, 1, 0, 0, 1, 1, 0], [0, 0, 1, 1, 0, 0, 1, 1], [0, 0, 0, 0, 1, 1, 1, 1]
+    T = np.zeros((24, 24))
+    for m in range(8):
+        for l in range(8):
+            s = 1
+            for a, pos in enumerate((cx[l], cy[l], cz[l])):
+                if (m >> a) & 1:
+                    s *= 1 if pos else -1
+            for c in range(3):
+                T[m * 3 + c, l * 3 + c] = s
+    return T
+
+
+@pytest.mark.parametrize("kind", ["cube", "box", "dense"])
+def test_matvec_element_operator_variants(lib, kind):
+    """The three element-operator code paths: cube elements (7 coefficients), isotropic
+    boxes (33 nonzero coefficients) and a reflection-symmetric K0 outside that pattern
+    (dense class blocks), each in FP64 and FP32 against the oracle."""
+    if kind == "cube":
+        K0 = unit_K0(3)
+    elif kind == "box":
+        K0 = unit_K0(3, nu=0.25, h=(1.0, 0.5, 2.0))
+    else:  # add a term coupling the x translations: class 1, row/column 0 becomes nonzero
+        Tm = _walsh_T()
+        dB = np.zeros((24, 24))
+        dB[0, 0] = 0.01
+        K0 = unit_K0(3) + Tm.T @ dB @ Tm
+    nel = (20, 9, 37)
+    rng = np.random.default_rng(11)
+    op = Op(lib, nel, K0)
+    E = rng.uniform(1e-3, 1.0, int(np.prod(nel)))
+    u = rng.standard_normal(op.ndof)
+    cons = rng.choice(op.ndof, size=op.ndof // 9, replace=False)
+    assert rel(op.matvec(E, u, cons), O.matvec(nel, K0, E, u, cons)) < 1e-12
+    y32 = op.matvec(E.astype(np.float32), u.astype(np.float32), cons, fp32=True)
+    assert rel(y32, O.matvec(nel, K0, E.astype(np.float32), u.astype(np.float32), cons)) < 2e-5
+
+
 def test_matvec_symmetric_and_deterministic(lib):
     nel = (24, 12, 20)
     rng = np.random.default_rng(7)
