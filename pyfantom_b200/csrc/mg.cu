@@ -44,7 +44,7 @@ struct Level {
     void* e = nullptr;  // coarse correction
     void* dinv = nullptr;
     double* A64 = nullptr;  // block stencil (level >= 1)
-    float* A32 = nullptr;
+    void* H = nullptr;      // its half storage in the V-cycle precision (smoothed levels)
 };
 
 }  // namespace pf
@@ -301,10 +301,7 @@ static int fine_mv(pf_mg* mg, const T* u, const Epi<T>& epi, cudaStream_t st) {
 template <typename T>
 static int level_matvec(pf_mg* mg, int l, const T* u, const Epi<T>& epi, cudaStream_t st) {
     if (l == 0) return fine_mv<T>(mg, u, epi, st);
-    if constexpr (sizeof(T) == 8)
-        return launch_stencil_matvec<double>(mg->L[l].g, mg->L[l].A64, u, epi, st);
-    else
-        return launch_stencil_matvec<float>(mg->L[l].g, mg->L[l].A32, u, epi, st);
+    return launch_stencil_matvec<T>(mg->L[l].g, (const T*)mg->L[l].H, u, epi, st, true);
 }
 
 template <typename T>
@@ -392,7 +389,7 @@ static void mg_free(pf_mg* mg) {
         Level& L = mg->L[l];
         for (void* p : {L.b, L.x, L.t, L.r, L.e, L.dinv}) if (p) cudaFree(p);
         if (L.A64) cudaFree(L.A64);
-        if (L.A32) cudaFree(L.A32);
+        if (L.H) cudaFree(L.H);
         L = Level();
     }
     dense_free(&mg->dense);
@@ -457,7 +454,7 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
         if (l >= 1) {
             const size_t nst = (size_t)gl.n_nodes * (gl.dim == 3 ? 27 : 9) * gl.dof * gl.dof;
             s = s ? s : dalloc((void**)&L.A64, nst * sizeof(double));
-            if (mg->fp32 && l < mg->nlev) s = s ? s : dalloc((void**)&L.A32, nst * sizeof(float));
+            if (l < mg->nlev) s = s ? s : dalloc(&L.H, (size_t)stencil_half_size(gl) * ts);
         }
         gl = coarse_grid(gl);
     }
@@ -569,9 +566,10 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
         const long long nst = L.g.n_nodes * (L.g.dim == 3 ? 27 : 9) * L.g.dof * L.g.dof;
         if (mg->fp32) {
             if ((s = launch_stencil_dinv<float>(L.g, L.A64, (float*)L.dinv, st))) return s;
-            if ((s = launch_d2f(nst, L.A64, L.A32, st))) return s;
+            if ((s = launch_stencil_half<float>(L.g, L.A64, (float*)L.H, st))) return s;
         } else {
             if ((s = launch_stencil_dinv<double>(L.g, L.A64, (double*)L.dinv, st))) return s;
+            if ((s = launch_stencil_half<double>(L.g, L.A64, (double*)L.H, st))) return s;
         }
     }
     // coarsest: dense factor and inverse

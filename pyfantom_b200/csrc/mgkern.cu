@@ -164,11 +164,16 @@ template int launch_prolong<float>(const Grid&, const float*, float*, const int*
 // all 32 nodes (coalesced reads of the structure-of-arrays coefficients), the per-warp
 // partial sums meet in shared memory and warp 0 adds them in a fixed order and applies the
 // epilogue.  3D: 9 warps x 3 offsets, 2D: 3 warps x 3 offsets.
+// HALF: A holds only the centre and the upper offsets o > c (c = NB/2 the centre, stored
+// block q = o - c); a lower offset o < c uses the symmetry of the level operator,
+// A[n, o] = A[n+o, -o]^T, i.e. block q = c - o of the neighbour n+o, transposed.  The
+// neighbour's coefficients are read again by another block shortly after (from L2), so
+// DRAM carries each coefficient once: (NB+1)/2 blocks per node instead of NB.
 // ---------------------------------------------------------------------------------------
-template <int DIM, typename T>
+template <int DIM, typename T, bool HALF>
 __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
                                                                         const T* __restrict__ u, Epi<T> epi) {
-    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM, NG = NB / 3;
+    constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM, NG = NB / 3, C = NB / 2;
     __shared__ T s_part[NG][DIM][32];
     if (epi.skip && *epi.skip) return;
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -190,10 +195,25 @@ __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<
             T um[DIM];
 #pragma unroll
             for (int b = 0; b < DIM; b++) um[b] = u[m * DIM + b];
+            if (!HALF) {
 #pragma unroll
-            for (int a = 0; a < DIM; a++)
+                for (int a = 0; a < DIM; a++)
 #pragma unroll
-                for (int b = 0; b < DIM; b++) acc[a] = fma(A[((long long)(o * BS + a * DIM + b)) * N + n], um[b], acc[a]);
+                    for (int b = 0; b < DIM; b++)
+                        acc[a] = fma(A[((long long)(o * BS + a * DIM + b)) * N + n], um[b], acc[a]);
+            } else if (o >= C) {
+                const T* Aq = A + (long long)(o - C) * BS * N + n;
+#pragma unroll
+                for (int a = 0; a < DIM; a++)
+#pragma unroll
+                    for (int b = 0; b < DIM; b++) acc[a] = fma(Aq[(long long)(a * DIM + b) * N], um[b], acc[a]);
+            } else {
+                const T* Aq = A + (long long)(C - o) * BS * N + m;
+#pragma unroll
+                for (int a = 0; a < DIM; a++)
+#pragma unroll
+                    for (int b = 0; b < DIM; b++) acc[a] = fma(Aq[(long long)(b * DIM + a) * N], um[b], acc[a]);
+            }
         }
     }
 #pragma unroll
@@ -221,20 +241,54 @@ __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<
 }
 
 template <typename T>
-int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st) {
+int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st, bool half) {
     const unsigned nb = (unsigned)((g.n_nodes + 31) / 32);
     pf::count_launch();
-    if (g.dim == 3)
-        k_stencil_matvec<3, T><<<nb, 288, 0, st>>>(gdev<3>(g), A, u, epi);
-    else
-        k_stencil_matvec<2, T><<<nb, 96, 0, st>>>(gdev<2>(g), A, u, epi);
+    if (g.dim == 3) {
+        if (half)
+            k_stencil_matvec<3, T, true><<<nb, 288, 0, st>>>(gdev<3>(g), A, u, epi);
+        else
+            k_stencil_matvec<3, T, false><<<nb, 288, 0, st>>>(gdev<3>(g), A, u, epi);
+    } else {
+        if (half)
+            k_stencil_matvec<2, T, true><<<nb, 96, 0, st>>>(gdev<2>(g), A, u, epi);
+        else
+            k_stencil_matvec<2, T, false><<<nb, 96, 0, st>>>(gdev<2>(g), A, u, epi);
+    }
     PF_LAUNCH_CHECK("stencil matvec launch");
     return PF_OK;
 }
 long long stencil_matvec_num_blocks(const Grid& g) { return (g.n_nodes + 31) / 32; }
 template int launch_stencil_matvec<double>(const Grid&, const double*, const double*, const Epi<double>&,
-                                           cudaStream_t);
-template int launch_stencil_matvec<float>(const Grid&, const float*, const float*, const Epi<float>&, cudaStream_t);
+                                           cudaStream_t, bool);
+template int launch_stencil_matvec<float>(const Grid&, const float*, const float*, const Epi<float>&, cudaStream_t,
+                                          bool);
+
+// half storage for the V-cycle: the centre and upper-offset blocks of the full FP64 stencil,
+// converted to the V-cycle precision
+template <typename T>
+__global__ void k_stencil_half(long long N, int nh, int bs, int c, const double* __restrict__ A, T* __restrict__ H) {
+    const long long total = N * nh * bs;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
+        H[i] = (T)A[i + (long long)c * bs * N];
+}
+long long stencil_half_size(const Grid& g) {
+    const int nb = g.dim == 3 ? 27 : 9;
+    return g.n_nodes * ((nb + 1) / 2) * g.dof * g.dof;
+}
+template <typename T>
+int launch_stencil_half(const Grid& g, const double* A, T* H, cudaStream_t st) {
+    const int nb = g.dim == 3 ? 27 : 9, bs = g.dof * g.dof;
+    const long long total = stencil_half_size(g);
+    long long blocks = (total + 255) / 256;
+    if (blocks > 8LL * kNumSM * 4) blocks = 8LL * kNumSM * 4;
+    pf::count_launch();
+    k_stencil_half<T><<<(unsigned)blocks, 256, 0, st>>>(g.n_nodes, (nb + 1) / 2, bs, nb / 2, A, H);
+    PF_LAUNCH_CHECK("stencil half launch");
+    return PF_OK;
+}
+template int launch_stencil_half<double>(const Grid&, const double*, double*, cudaStream_t);
+template int launch_stencil_half<float>(const Grid&, const double*, float*, cudaStream_t);
 
 // ---------------------------------------------------------------------------------------
 // Galerkin level 1 from the element operator.

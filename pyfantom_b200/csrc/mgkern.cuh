@@ -9,8 +9,13 @@ template <typename TI, typename TO>
 int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st);
 template <typename T>
 int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st);
+// half = true: A is the half storage of launch_stencil_half (centre and upper offsets)
 template <typename T>
-int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st);
+int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st,
+                          bool half = false);
+long long stencil_half_size(const Grid& g);  // elements of the half storage
+template <typename T>
+int launch_stencil_half(const Grid& g, const double* A, T* H, cudaStream_t st);
 long long stencil_matvec_num_blocks(const Grid& g);
 
 void galerkin_child_matrices(int dim, const double* K0, double* Kc);
