@@ -121,6 +121,10 @@ int op_factorise(Op* op) {
 // ---------------------------------------------------------------------------------------
 // 3D matvec: x-marching tile kernel
 // ---------------------------------------------------------------------------------------
+// nodes owned per warp along z: FP32 (register staging) 30 of 32 loaded node columns,
+// FP64 (cp.async staging of 33 columns) 31
+constexpr int kZTile32 = 30, kZTile64 = 31;
+
 template <typename T>
 struct H8Blk {
     T b[8][3][3];
@@ -149,24 +153,26 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Pipelined x-march.  Step s (element layer ie = ix0-1+s):
-//   1. cp.async the node plane ie+2 into plane buffer s&1 (last read in step s-1) and this
-//      thread's epilogue operands for its node of plane ie into its private slots;
+//   1. cp.async this thread's epilogue operands for its node of plane ie into its slots;
 //   2. forward stages of the plane ie+1 face (buffer (s+1)&1), element operator, inverse
 //      stages, node sums inside the warp (shuffles), exchange row sums in s_x[s&1];
-//   3. wait for this thread's copies, zero the constrained components it copied,
+//   3. publish plane ie+2 (in registers since the previous step) to buffer s&1 (last read
+//      in step s-1), start loading plane ie+3, wait for the epilogue copies,
 //      __syncthreads (the only barrier of the step);
 //   4. owners finish their node of plane ie and apply the epilogue.
 // CM selects the element operator: 0 dense class blocks read from shared memory (any K0
 // with the reflection symmetry), 1 the 33 nonzeros of an isotropic box element, 2 the 7
 // values of a cube element (1, 2: coefficients held in registers).
 template <typename T, typename TE, int TY, int CM>
-__global__ void __launch_bounds__((TY + 1) * 32)
+__global__ void __launch_bounds__((TY + 1) * 32, 3)
     k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
                 const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
     constexpr int NW = TY + 1;
     constexpr int NT = NW * 32;
     constexpr int PR = TY + 2, PC = 33, NPE = PR * PC;
-    constexpr int NQ = (NPE + NT - 1) / NT;  // plane entries per thread
+    constexpr int NQ = (NPE + NT - 1) / NT;   // plane entries per thread (cp.async staging)
+    constexpr bool RS = sizeof(T) == 4;       // register staging (FP32) or cp.async (FP64)
+    constexpr int ZT = RS ? kZTile32 : kZTile64;
     constexpr int NSLOT = 6;                 // u (identity rows), b, x, dinv, xadd, dot_a
     __shared__ __align__(16) T s_u[2][3][PR][PC];
     __shared__ T s_x[2][3][NW][32];
@@ -176,11 +182,11 @@ __global__ void __launch_bounds__((TY + 1) * 32)
     if (epi.skip && *epi.skip) return;
     const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int kz0 = blockIdx.x * 31, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
+    const int kz0 = blockIdx.x * ZT, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
     const int je = jy0 - 1 + w, ke = kz0 - 1 + l;
     const int jn = jy0 + w, kn = kz0 + l;
-    const bool owner = (w < TY) && (l < 31) && (jn < ny) && (kn < nz);
-    const bool col_ok = (je >= 0) && (je < NY) && (ke >= 0) && (ke < NZ);
+    const bool owner = (w < TY) && (l < ZT) && (jn < ny) && (kn < nz);
+    const bool col_ok = (l <= ZT) && (je >= 0) && (je < NY) && (ke >= 0) && (ke < NZ);
     const T wgt = epi_omega(epi);
     const int mode = epi.mode;
     const bool need_b = mode != PF_EPI_STORE, need_d = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
@@ -188,8 +194,9 @@ __global__ void __launch_bounds__((TY + 1) * 32)
     double dot = 0.0;
     constexpr int TB_ = (int)sizeof(T);
 
+    // FP64: cp.async copies of whole plane tiles (33 node columns, 31 owned per warp).
     // issue the copies of plane p into buffer buf; returns the masks of the entries issued
-    auto issue_plane = [&](int p, int buf, uint8_t* mq) {
+    [[maybe_unused]] auto issue_plane = [&](int p, int buf, uint8_t* mq) {
 #pragma unroll
         for (int q = 0; q < NQ; q++) {
             const int idx = tid + q * NT;
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__((TY + 1) * 32)
             }
         }
     };
-    auto fix_plane = [&](int buf, const uint8_t* mq) {
+    [[maybe_unused]] auto fix_plane = [&](int buf, const uint8_t* mq) {
 #pragma unroll
         for (int q = 0; q < NQ; q++) {
             const int idx = tid + q * NT;
@@ -219,6 +226,50 @@ __global__ void __launch_bounds__((TY + 1) * 32)
                 for (int d = 0; d < 3; d++)
                     if (mq[q] & (1 << d)) s_u[buf][d][r][c] = T(0);
             }
+        }
+    };
+    // FP32: plane staging through registers: thread (w, l) loads node (jy0 - 1 + w, kz0 - 1 + l) of a plane into
+    // registers one step ahead (coalesced: a warp reads 32 consecutive nodes), zeroes its
+    // constrained components (skipped columns) and publishes it to row w, column l of a
+    // plane buffer; the last warp also carries the row jy0 + TY above the tile.  Lanes
+    // 0..30 compute the elements kz0-1 .. kz0+29 and own the nodes kz0 .. kz0+29; lane 31
+    // is inactive and reads column 32, which is zero and never written.
+    const int jo = jy0 - 1 + w, ko = kz0 - 1 + l, jx = jy0 + TY;
+    const bool own_ok = jo >= 0 && jo < ny && ko >= 0 && ko < nz;
+    const bool ext_ok = jx < ny && ko >= 0 && ko < nz;
+    T rv[3], rx[3];
+    uint8_t rm = 0, rxm = 0;
+    [[maybe_unused]] auto load_plane = [&](int p) {
+        const bool pok = p >= 0 && p < nx;
+        rm = 0;
+        if (pok && own_ok) {
+            const long long n = (long long)ko + (long long)nz * (p + (long long)nx * jo);
+            if (mask) rm = mask[n];
+#pragma unroll
+            for (int d = 0; d < 3; d++) rv[d] = u[3 * n + d];
+        } else {
+#pragma unroll
+            for (int d = 0; d < 3; d++) rv[d] = T(0);
+        }
+        if (w == TY) {
+            rxm = 0;
+            if (pok && ext_ok) {
+                const long long n = (long long)ko + (long long)nz * (p + (long long)nx * jx);
+                if (mask) rxm = mask[n];
+#pragma unroll
+                for (int d = 0; d < 3; d++) rx[d] = u[3 * n + d];
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; d++) rx[d] = T(0);
+            }
+        }
+    };
+    [[maybe_unused]] auto publish = [&](int buf) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) s_u[buf][d][w][l] = ((rm >> d) & 1) ? T(0) : rv[d];
+        if (w == TY) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) s_u[buf][d][TY + 1][l] = ((rxm >> d) & 1) ? T(0) : rx[d];
         }
     };
     auto face = [&](int buf, T g[3][2][2]) {
@@ -243,16 +294,25 @@ __global__ void __launch_bounds__((TY + 1) * 32)
     // held in 72 (FP32) / 144 (FP64) registers for the whole kernel
     const volatile T* vb = s_blk;
 #define BK(p, i, j) vb[(p) * 9 + (i) * 3 + (j)]
-    // prologue: planes ix0-1 (buffer 0) and ix0 (buffer 1)
-    uint8_t mq[NQ];
-    issue_plane(ix0 - 1, 0, mq);
-    cp_async_commit();
-    cp_async_wait_all();
-    fix_plane(0, mq);
-    issue_plane(ix0, 1, mq);
-    cp_async_commit();
-    cp_async_wait_all();
-    fix_plane(1, mq);
+    // prologue: planes ix0-1 (buffer 0) and ix0 (buffer 1); FP32: plane ix0+1 in flight
+    [[maybe_unused]] uint8_t mq[NQ];
+    if constexpr (RS) {
+        if (tid < 2 * 3 * PR) (&s_u[0][0][0][0])[tid * PC + 32] = T(0);
+        load_plane(ix0 - 1);
+        publish(0);
+        load_plane(ix0);
+        publish(1);
+        load_plane(ix0 + 1);
+    } else {
+        issue_plane(ix0 - 1, 0, mq);
+        cp_async_commit();
+        cp_async_wait_all();
+        fix_plane(0, mq);
+        issue_plane(ix0, 1, mq);
+        cp_async_commit();
+        cp_async_wait_all();
+        fix_plane(1, mq);
+    }
     __syncthreads();
     T glo[3][2][2], carry[3][2][2];
     face(0, glo);
@@ -269,8 +329,8 @@ __global__ void __launch_bounds__((TY + 1) * 32)
     for (int s = 0; s <= CXc; s++) {
         const int ie = ix0 - 1 + s;
         const int cur = (s + 1) & 1;
-        // 1. asynchronous copies
-        issue_plane(ie + 2, s & 1, mq);
+        // 1. asynchronous copies (FP64: plane ie+2 into buffer s&1) and epilogue operands
+        if constexpr (!RS) issue_plane(ie + 2, s & 1, mq);
         const bool out_now = owner && s >= 1 && ie < nx;
         long long n_out = 0;
         uint8_t m_out = 0;
@@ -405,9 +465,16 @@ __global__ void __launch_bounds__((TY + 1) * 32)
             const T P0 = t[c][0][1] + __shfl_down_sync(0xffffffffu, t[c][0][0], 1);
             s_x[s & 1][c][w][l] = P0;
         }
-        // 3. copies landed, constrained components zeroed, one barrier
-        cp_async_wait_all();
-        fix_plane(s & 1, mq);
+        // 3. FP32: publish plane ie+2 (loaded during the previous step), load plane ie+3;
+        //    FP64: zero the constrained components of the copied plane; one barrier
+        if constexpr (RS) {
+            publish(s & 1);
+            load_plane(ie + 3);
+            cp_async_wait_all();
+        } else {
+            cp_async_wait_all();
+            fix_plane(s & 1, mq);
+        }
         __syncthreads();
         // 4. owners finish their node of plane ie
         if (out_now) {
@@ -456,7 +523,8 @@ constexpr int kTY32 = 8;  // FP32: 9 warps per block
 
 static void h8_launch_dims(const Grid& g, int TY, dim3* grid, int* CXc) {
     const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
-    const int tz = (nz + 30) / 31, ty = (ny + TY - 1) / TY;
+    const int zt = TY == kTY32 ? kZTile32 : kZTile64;
+    const int tz = (nz + zt - 1) / zt, ty = (ny + TY - 1) / TY;
     // enough x-chunks for ~4 waves of blocks, chunks of 4..32 planes
     const long long target = 4LL * kNumSM * 3;
     int chunks = (int)((target + (long long)tz * ty - 1) / ((long long)tz * ty));
