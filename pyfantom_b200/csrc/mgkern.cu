@@ -67,72 +67,86 @@ static GridDev<DIM> gdev(const Grid& g) {
 // ---------------------------------------------------------------------------------------
 // transfers
 // ---------------------------------------------------------------------------------------
+// One thread per (coarse node, component): the 3^DIM weighted fine values of that
+// component, accumulated in the output precision.  Per axis the weights are 0.5 / 1 / 0.5
+// and 1/tw factorises into 1/1.5 (boundary node) or 1/2.
 template <int DIM, typename TI, typename TO>
 __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restrict__ vf, TO* __restrict__ vc,
                            const int* skip) {
+    using TA = TO;  // accumulation precision
     if (skip && *skip) return;
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= gc.n_nodes) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= gc.n_nodes * DIM) return;
+    const long long c = t / DIM;
+    const int d = (int)(t - c * DIM);
     int ic, jc, kc;
     ndec(gc, c, ic, jc, kc);
-    const double inv_tw = 1.0 / total_weight(gc, ic, jc, kc);
-    double acc[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; d++) acc[d] = 0.0;
+    const int fi = 2 * ic, fj = 2 * jc, fk = 2 * kc;
+    const TA ti = (ic == 0 || ic == gc.nn[0] - 1) ? TA(1.0 / 1.5) : TA(0.5);
+    const TA tj = (jc == 0 || jc == gc.nn[1] - 1) ? TA(1.0 / 1.5) : TA(0.5);
+    TA tk = TA(1);
+    if (DIM == 3) tk = (kc == 0 || kc == gc.nn[2] - 1) ? TA(1.0 / 1.5) : TA(0.5);
     constexpr int KR = DIM == 3 ? 1 : 0;
+    TA acc = TA(0);
 #pragma unroll
-    for (int di = -1; di <= 1; di++)
+    for (int dj = -1; dj <= 1; dj++) {
+        const int j = fj + dj;
+        if (j < 0 || j >= gf.nn[1]) continue;
+        TA accj = TA(0);
 #pragma unroll
-        for (int dj = -1; dj <= 1; dj++)
+        for (int di = -1; di <= 1; di++) {
+            const int i = fi + di;
+            if (i < 0 || i >= gf.nn[0]) continue;
+            TA acci = TA(0);
 #pragma unroll
             for (int dk = -KR; dk <= KR; dk++) {
-                const int fi = 2 * ic + di, fj = 2 * jc + dj, fk = 2 * kc + dk;
-                if (!nok(gf, fi, fj, fk)) continue;
-                const double w = half_pow((di != 0) + (dj != 0) + (dk != 0));
-                const long long n = nidx(gf, fi, fj, fk);
-#pragma unroll
-                for (int d = 0; d < DIM; d++) acc[d] += w * (double)vf[n * DIM + d];
+                const int k = fk + dk;
+                if (DIM == 3 && (k < 0 || k >= gf.nn[2])) continue;
+                const TA v = (TA)vf[nidx(gf, i, j, k) * DIM + d];
+                acci += dk == 0 ? v : TA(0.5) * v;
             }
-#pragma unroll
-    for (int d = 0; d < DIM; d++) vc[c * DIM + d] = (TO)(acc[d] * inv_tw);
+            accj += di == 0 ? acci : TA(0.5) * acci;
+        }
+        acc += dj == 0 ? accj : TA(0.5) * accj;
+    }
+    vc[c * DIM + d] = (TO)(acc * ti * tj * tk);
 }
 
+// One thread per (fine node, component): P = Phat diag(1/tw), the mean of the 1, 2, 4 or 8
+// parent values divided by their tw.
 template <int DIM, typename T>
 __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict__ vc, T* __restrict__ vf,
                           const int* skip) {
     if (skip && *skip) return;
-    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= gf.n_nodes) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= gf.n_nodes * DIM) return;
+    const long long f = t / DIM;
+    const int d = (int)(t - f * DIM);
     int i, j, k;
     ndec(gf, f, i, j, k);
-    double acc[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; d++) acc[d] = 0.0;
-    int count = 0;
-    const int k0 = DIM == 3 ? k / 2 : 0, k1 = DIM == 3 ? k / 2 + (k & 1) : 0;
-    for (int ci = i / 2; ci <= i / 2 + (i & 1); ci++) {
-        if (ci >= gc.nn[0]) continue;
-        for (int cj = j / 2; cj <= j / 2 + (j & 1); cj++) {
-            if (cj >= gc.nn[1]) continue;
+    const int i0 = i >> 1, j0 = j >> 1, k0 = DIM == 3 ? k >> 1 : 0;
+    const int i1 = i0 + (i & 1), j1 = j0 + (j & 1), k1 = DIM == 3 ? k0 + (k & 1) : 0;
+    auto itw = [&](int c, int n) { return (c == 0 || c == n - 1) ? T(1.0 / 1.5) : T(0.5); };
+    T acc = T(0);
+    for (int cj = j0; cj <= j1; cj++) {
+        const T wj = itw(cj, gc.nn[1]);
+        for (int ci = i0; ci <= i1; ci++) {
+            const T wij = wj * itw(ci, gc.nn[0]);
             for (int ck = k0; ck <= k1; ck++) {
-                if (DIM == 3 && ck >= gc.nn[2]) continue;
-                const double itw = 1.0 / total_weight(gc, ci, cj, ck);
-                const long long n = nidx(gc, ci, cj, ck);
-#pragma unroll
-                for (int d = 0; d < DIM; d++) acc[d] += (double)vc[n * DIM + d] * itw;
-                count++;
+                const T w = DIM == 3 ? wij * itw(ck, gc.nn[2]) : wij;
+                acc += w * vc[nidx(gc, ci, cj, ck) * DIM + d];
             }
         }
     }
-    const double ic = count > 0 ? 1.0 / count : 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) vf[f * DIM + d] = (T)(acc[d] * ic);
+    const int nodd = (i & 1) + (j & 1) + (DIM == 3 ? (k & 1) : 0);
+    const T scale = nodd == 0 ? T(1) : nodd == 1 ? T(0.5) : nodd == 2 ? T(0.25) : T(0.125);
+    vf[f * DIM + d] = acc * scale;
 }
 
 template <typename TI, typename TO>
 int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st) {
     const Grid gc = coarse_grid(gf);
-    const unsigned nb = (unsigned)((gc.n_nodes + 255) / 256);
+    const unsigned nb = (unsigned)((gc.n_nodes * gf.dim + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
         k_restrict<3, TI, TO><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vf, vc, skip);
@@ -144,7 +158,7 @@ int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaS
 template <typename T>
 int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st) {
     const Grid gc = coarse_grid(gf);
-    const unsigned nb = (unsigned)((gf.n_nodes + 255) / 256);
+    const unsigned nb = (unsigned)((gf.n_nodes * gf.dim + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
         k_prolong<3, T><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vc, vf, skip);
