@@ -164,7 +164,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // with the reflection symmetry), 1 the 33 nonzeros of an isotropic box element, 2 the 7
 // values of a cube element (1, 2: coefficients held in registers).
 template <typename T, typename TE, int TY, int CM>
-__global__ void __launch_bounds__((TY + 1) * 32, sizeof(T) == 4 ? 3 : 1)
+__global__ void __launch_bounds__((TY + 1) * 32, 3)
     k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
                 const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
     constexpr int NW = TY + 1;
