@@ -668,14 +668,15 @@ __global__ void k_diagonal(Grid g, const double* __restrict__ E, const uint8_t* 
     if (n >= g.n_nodes) return;
     const int dof = g.dim, nc = g.dim == 3 ? 8 : 4;
     int i, j, k;
+    const unsigned un = (unsigned)n;  // fewer than 2^31 nodes (validate_grid)
     if (g.dim == 3) {
-        k = (int)(n % g.nn[2]);
-        const long long t = n / g.nn[2];
-        i = (int)(t % g.nn[0]);
-        j = (int)(t / g.nn[0]);
+        const unsigned t = un / (unsigned)g.nn[2];
+        k = (int)(un - t * (unsigned)g.nn[2]);
+        j = (int)(t / (unsigned)g.nn[0]);
+        i = (int)(t - (unsigned)j * (unsigned)g.nn[0]);
     } else {
-        i = (int)(n % g.nn[0]);
-        j = (int)(n / g.nn[0]);
+        j = (int)(un / (unsigned)g.nn[0]);
+        i = (int)(un - (unsigned)j * (unsigned)g.nn[0]);
         k = 0;
     }
     const uint8_t m = mask ? mask[n] : (uint8_t)0;

@@ -37,13 +37,15 @@ __global__ void __launch_bounds__(256) k_filter(int nelx, int nely, int nelz, in
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     int i, j, k = 0;
+    const unsigned ue = (unsigned)e;  // element counts stay below 2^31 (validate_grid)
     if (DIM == 3) {
-        i = (int)(e / ((long long)nely * nelz));
-        j = (int)((e / nelz) % nely);
-        k = (int)(e % nelz);
+        const unsigned t = ue / (unsigned)nelz;
+        k = (int)(ue - t * (unsigned)nelz);
+        i = (int)(t / (unsigned)nely);
+        j = (int)(t - (unsigned)i * (unsigned)nely);
     } else {
-        i = (int)(e / nely);
-        j = (int)(e % nely);
+        i = (int)(ue / (unsigned)nely);
+        j = (int)(ue - (unsigned)i * (unsigned)nely);
     }
     double sv = 0.0, sw = 0.0;
     for (int t = 0; t < K; t++) {

@@ -26,16 +26,21 @@ __host__ __device__ __forceinline__ long long nidx(const GridDev<DIM>& g, int i,
     if (DIM == 3) return (long long)k + (long long)g.nn[2] * (i + (long long)g.nn[0] * j);
     return (long long)i + (long long)g.nn[0] * j;
 }
+// node index -> (i, j, k); 32-bit unsigned division (grids hold fewer than 2^31 DOFs,
+// checked by validate_grid), far cheaper than the emulated 64-bit one
 template <int DIM>
 __device__ __forceinline__ void ndec(const GridDev<DIM>& g, long long n, int& i, int& j, int& k) {
+    const unsigned un = (unsigned)n;
     if (DIM == 3) {
-        k = (int)(n % g.nn[2]);
-        const long long t = n / g.nn[2];
-        i = (int)(t % g.nn[0]);
-        j = (int)(t / g.nn[0]);
+        const unsigned nz = (unsigned)g.nn[2], nx = (unsigned)g.nn[0];
+        const unsigned t = un / nz;
+        k = (int)(un - t * nz);
+        j = (int)(t / nx);
+        i = (int)(t - (unsigned)j * nx);
     } else {
-        i = (int)(n % g.nn[0]);
-        j = (int)(n / g.nn[0]);
+        const unsigned nx = (unsigned)g.nn[0];
+        j = (int)(un / nx);
+        i = (int)(un - (unsigned)j * nx);
         k = 0;
     }
 }
@@ -77,7 +82,7 @@ __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restric
     if (skip && *skip) return;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= gc.n_nodes * DIM) return;
-    const long long c = t / DIM;
+    const long long c = (unsigned)t / DIM;
     const int d = (int)(t - c * DIM);
     int ic, jc, kc;
     ndec(gc, c, ic, jc, kc);
@@ -120,7 +125,7 @@ __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict_
     if (skip && *skip) return;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= gf.n_nodes * DIM) return;
-    const long long f = t / DIM;
+    const long long f = (unsigned)t / DIM;
     const int d = (int)(t - f * DIM);
     int i, j, k;
     ndec(gf, f, i, j, k);
