@@ -326,7 +326,8 @@ static Epi<T> make_epi(int mode, const T* b, const T* x, const T* dinv, const T*
 // Approximate A_l x = b from x = 0; returns (through *res) the buffer holding x.
 // b0 overrides the level-0 right-hand side.  dot: optional fused r.z partial at level 0.
 template <typename T>
-static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, const double* dot_a, cudaStream_t st) {
+static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, const double* dot_a, cudaStream_t st,
+                  bool x_ready = false) {
     Level& L = mg->L[l];
     const int* skip = &mg->st->done;
     const double* omega = &mg->st->omega;
@@ -341,9 +342,11 @@ static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, 
     T* X = (T*)L.x;
     T* Tb = (T*)L.t;
     int s;
-    pf::count_launch();
-    k_jacobi0<T><<<vec_blocks(L.ndof), kRedThreads, 0, st>>>(L.ndof, b, dinv, omega, scale, X, skip);
-    PF_LAUNCH_CHECK("jacobi0 launch");
+    if (!x_ready) {  // otherwise the restriction from the finer level did this sweep
+        pf::count_launch();
+        k_jacobi0<T><<<vec_blocks(L.ndof), kRedThreads, 0, st>>>(L.ndof, b, dinv, omega, scale, X, skip);
+        PF_LAUNCH_CHECK("jacobi0 launch");
+    }
     for (int k = 1; k < mg->cfg.n_smooth; k++) {
         if ((s = level_matvec<T>(mg, l, X, make_epi<T>(PF_EPI_JACOBI, b, X, dinv, nullptr, Tb, omega, scale, skip), st)))
             return s;
@@ -354,9 +357,17 @@ static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, 
     T* R = (T*)L.r;
     if ((s = level_matvec<T>(mg, l, X, make_epi<T>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, R, omega, scale, skip), st)))
         return s;
-    if ((s = launch_restrict<T, T>(L.g, R, (T*)mg->L[l + 1].b, skip, st))) return s;
+    Jacobi0<T> j0;
+    const bool fuse = l + 1 < mg->nlev;  // the coarsest level is solved directly
+    if (fuse) {
+        j0.x = (T*)mg->L[l + 1].x;
+        j0.dinv = (const T*)mg->L[l + 1].dinv;
+        j0.omega = omega;
+        j0.scale = pow(mg->cfg.omega_boost, l + 1);
+    }
+    if ((s = launch_restrict<T, T>(L.g, R, (T*)mg->L[l + 1].b, skip, st, j0))) return s;
     T* ec;
-    if ((s = vcycle<T>(mg, l + 1, nullptr, &ec, nullptr, nullptr, st))) return s;
+    if ((s = vcycle<T>(mg, l + 1, nullptr, &ec, nullptr, nullptr, st, fuse))) return s;
     T* Eb = (T*)L.e;
     if ((s = launch_prolong<T>(L.g, ec, Eb, skip, st))) return s;
     for (int k = 0; k < mg->cfg.n_smooth; k++) {

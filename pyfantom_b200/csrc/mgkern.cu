@@ -77,7 +77,7 @@ static GridDev<DIM> gdev(const Grid& g) {
 // and 1/tw factorises into 1/1.5 (boundary node) or 1/2.
 template <int DIM, typename TI, typename TO>
 __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restrict__ vf, TO* __restrict__ vc,
-                           const int* skip) {
+                           const int* skip, Jacobi0<TO> j0) {
     using TA = TO;  // accumulation precision
     if (skip && *skip) return;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -114,7 +114,10 @@ __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restric
         }
         acc += dj == 0 ? accj : TA(0.5) * accj;
     }
-    vc[c * DIM + d] = (TO)(acc * ti * tj * tk);
+    const TO bc = (TO)(acc * ti * tj * tk);
+    vc[c * DIM + d] = bc;
+    // first smoothing sweep of the coarse level from x = 0: x = omega * scale / diag * b
+    if (j0.x) j0.x[c * DIM + d] = (TO)((*j0.omega) * j0.scale) * j0.dinv[c * DIM + d] * bc;
 }
 
 // One thread per (fine node, component): P = Phat diag(1/tw), the mean of the 1, 2, 4 or 8
@@ -149,14 +152,14 @@ __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict_
 }
 
 template <typename TI, typename TO>
-int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st) {
+int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st, Jacobi0<TO> j0) {
     const Grid gc = coarse_grid(gf);
     const unsigned nb = (unsigned)((gc.n_nodes * gf.dim + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
-        k_restrict<3, TI, TO><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vf, vc, skip);
+        k_restrict<3, TI, TO><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0);
     else
-        k_restrict<2, TI, TO><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), vf, vc, skip);
+        k_restrict<2, TI, TO><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), vf, vc, skip, j0);
     PF_LAUNCH_CHECK("restrict launch");
     return PF_OK;
 }
@@ -172,8 +175,10 @@ int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStre
     PF_LAUNCH_CHECK("prolong launch");
     return PF_OK;
 }
-template int launch_restrict<double, double>(const Grid&, const double*, double*, const int*, cudaStream_t);
-template int launch_restrict<float, float>(const Grid&, const float*, float*, const int*, cudaStream_t);
+template int launch_restrict<double, double>(const Grid&, const double*, double*, const int*, cudaStream_t,
+                                            Jacobi0<double>);
+template int launch_restrict<float, float>(const Grid&, const float*, float*, const int*, cudaStream_t,
+                                          Jacobi0<float>);
 template int launch_prolong<double>(const Grid&, const double*, double*, const int*, cudaStream_t);
 template int launch_prolong<float>(const Grid&, const float*, float*, const int*, cudaStream_t);
 

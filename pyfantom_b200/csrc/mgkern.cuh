@@ -5,8 +5,17 @@
 
 namespace pf {
 
+// optional fused first Jacobi sweep of the coarse level: x = omega * scale * dinv * b_c
+template <typename T>
+struct Jacobi0 {
+    T* x = nullptr;
+    const T* dinv = nullptr;
+    const double* omega = nullptr;
+    double scale = 1.0;
+};
 template <typename TI, typename TO>
-int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st);
+int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st,
+                    Jacobi0<TO> j0 = Jacobi0<TO>());
 template <typename T>
 int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st);
 // half = true: A is the half storage of launch_stencil_half (centre and upper offsets)
