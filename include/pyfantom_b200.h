@@ -248,6 +248,23 @@ size_t pf_cnn_energy_loss_workspace(void);
 int pf_cnn_energy_loss_f64(long long n, const double* y, const double* Ky, const double* b, double c, float* grad,
                            double* loss, double* work, void* stream);
 
+/* ---- PGD (pyFANTOM/Optimizers/CUDA/PGD.py:6-372), single volume constraint ---------- */
+size_t pf_pgd_workspace_size(long long n); /* doubles, for both calls below */
+/* h_out[8] (host) = {df.df, max|df|, df.df_last, df_last.df_last, s.y, s.s, y.y, max|y|}
+ * with s = x_last - x, y = df_last - df (PGD.alpha, :107-142); x_last, df_last may both
+ * be NULL (first iteration: entries 2..7 are 0). */
+int pf_pgd_stats_f64(long long n, const double* x, const double* df, const double* x_last, const double* df_last,
+                     double* work, double* h_out, void* stream);
+/* d = -df + beta d_last (d_last NULL: d = -df), x_new = x + alpha d (PGD.iter, :226-236) */
+int pf_pgd_step_f64(long long n, const double* x, const double* df, const double* d_last, double beta, double alpha,
+                    double* d, double* x_new, void* stream);
+/* x_new = clip(xs + l dg, lo, hi) with l from the reference bisection on dg.x - vf <= 0
+ * (project_to_feasible, :144-170: l in [-1e12, 0], midpoint rule, stop when
+ * (l2-l1)/(l2+l1) <= tol, l = 0 when clip(xs) is feasible).  h_out (host, may be NULL)
+ * = {l, bisection steps, feasible at l = 0}. */
+int pf_pgd_project_f64(long long n, const double* xs, const double* dg, double vf, double lo, double hi, double tol,
+                       double* x_new, double* work, double* h_out, void* stream);
+
 /* ---- OC update without allocation --------------------------------------------------
  * No counterpart in the reference.  Same computation and outputs as pf_oc_update_f64,
  * for callers that cannot allocate device memory where they run the OC step (code being

@@ -306,6 +306,28 @@ def oc_update(x, df, dg, vf, move):
     return out, int(steps)
 
 
+def pgd_project(xs, dg, vf, lo=0.0, hi=1.0, tol=1e-8):
+    """The reference PGD projection for one volume constraint
+    (pyFANTOM/Optimizers/CPU/PGD.py:144-170): clip(xs + l dg, lo, hi) with l bisected in
+    [-1e12, 0] (midpoint rule, l2 = mid when dg.x - vf <= 0, else l1 = mid) until
+    (l2 - l1) / (l2 + l1) <= tol; returns (x_new, l, steps)."""
+    xs, dg = np.asarray(xs, np.float64), np.asarray(dg, np.float64)
+    l1, l2 = 0.0, -1e12
+    d = np.clip(xs + l1 * dg, lo, hi)
+    if dg @ d - vf <= 0.0:
+        return d, 0.0, 0
+    steps, lm = 0, 0.0
+    while (l2 - l1) / (l2 + l1) > tol:
+        lm = (l1 + l2) / 2
+        d = np.clip(xs + lm * dg, lo, hi)
+        if dg @ d - vf <= 0.0:
+            l2 = lm
+        else:
+            l1 = lm
+        steps += 1
+    return d, lm, steps
+
+
 def penalize(rho, penalty=3.0, void=1e-9, E_mul=1.0, heavyside=False, beta=2.0, eta=0.5):
     """SIMP law, Problem/CUDA/MinimumCompliance.py:305-324 (single material)."""
     rho = np.asarray(rho, dtype=np.float64)

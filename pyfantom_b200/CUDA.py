@@ -12,9 +12,9 @@ from .stiffness import StructuredStiffnessKernel  # noqa: F401
 from .solvers import CG, MultiGrid  # noqa: F401
 from .FiniteElement import FiniteElement  # noqa: F401
 from .Problem import MinimumCompliance  # noqa: F401
-from .Optimizers import OC  # noqa: F401
+from .Optimizers import OC, PGD  # noqa: F401
 from .physics import LinearElasticity  # noqa: F401
 
 __all__ = ["StructuredMesh2D", "StructuredMesh3D", "StructuredFilter2D", "StructuredFilter3D",
-           "StructuredStiffnessKernel", "CG", "MultiGrid", "FiniteElement", "MinimumCompliance", "OC",
+           "StructuredStiffnessKernel", "CG", "MultiGrid", "FiniteElement", "MinimumCompliance", "OC", "PGD",
            "LinearElasticity"]

@@ -10,6 +10,8 @@ five bisection levels per sweep over the elements, no host round trip per step).
 from __future__ import annotations
 
 import ctypes
+import math
+import sys
 import time
 
 import torch
@@ -17,7 +19,7 @@ import torch
 from . import _lib
 from ._tensor import device
 
-__all__ = ["Optimizer", "OC"]
+__all__ = ["Optimizer", "OC", "PGD"]
 
 
 class Optimizer:
@@ -87,6 +89,164 @@ class OC(Optimizer):
         self.change_f = float(torch.abs((f - self.last_f) / f))
         self.last_f = f
         self.last_desvars = x_new.clone()
+        if self.timer:
+            return end - start
+
+    def converged(self, *args, **kwargs):
+        if not self.problem.is_terminal():
+            return False
+        return self.change <= self.change_tol and self.change_f <= self.fun_tol
+
+    def logs(self):
+        return {"objective": float(self.last_f), "variable change": float(self.change),
+                "function change": float(self.change_f), **self.problem.logs()}
+
+
+class PGD(Optimizer):
+    """Projected gradient descent (drop-in for pyFANTOM/Optimizers/CUDA/PGD.py:6-372).
+
+    Same constructor arguments, ``iter``, ``converged`` and ``logs`` as the reference.  One
+    iteration: a Barzilai-Borwein step size from the gradient history with the reference's
+    safeguards and fall-backs (PGD.alpha, :107-142), optionally along conjugate directions
+    (beta = max(dx_n.(dx_n - dx_n-1) / |dx_n-1|^2, 0) with dx = -df), the step
+    x + alpha d, then the projection onto the volume constraint by the reference's bisection
+    for the shift l of clip(x + l dg, 0, 1) (:144-170).  The vector work runs in the
+    library (``pf_pgd_stats_f64``: the eight dot products and maxima of the step-size rule
+    in one pass; ``pf_pgd_step_f64``; ``pf_pgd_project_f64``: the bisection on the device,
+    five levels per sweep); the scalar rule is evaluated on the host exactly as written in
+    the reference.  Only the single-constraint path (``problem.m() == 1``, the reference's
+    ``is_independent or m == 1`` branch) is provided: the multi-constraint Newton /
+    Wolfe-line-search projection belongs to multi-material problems, which this library
+    does not build.
+    """
+
+    def __init__(self, problem, change_tol=1e-4, fun_tol=1e-6, maxiter_N=50, tol_B=1e-8, tol_N=1e-6, C=1e12,
+                 fall_back_move=0.2, alpha_max=1e2, relaxation=1.0, warmup_iter=50, timer=False,
+                 conjugate_directions=True):
+        super().__init__(problem)
+        self.last_desvars = problem.get_desvars().clone()
+        self.last_f = problem.f()
+        self.last_nabla_f = problem.nabla_f().clone()
+        self.m = problem.m()
+        if self.m != 1:
+            raise NotImplementedError("PGD here supports a single volume constraint (problem.m() == 1)")
+        self.lambda_map = problem.constraint_map()
+        self.bounds = problem.bounds()
+        self.change = float("inf")
+        self.change_f = float("inf")
+        self.change_tol = change_tol
+        self.fun_tol = fun_tol
+        self.tol_B = tol_B
+        self.tol_N = tol_N
+        self.C = C
+        self.fall_back_move = fall_back_move
+        self.alpha_max = alpha_max
+        self.maxiter_N = maxiter_N
+        self.timer = timer
+        self.relaxation = relaxation
+        self.warmup_iter = warmup_iter
+        self.conjugate = conjugate_directions
+        self.iteration = 0
+        self.is_independent = problem.is_independent()
+        self.d_last = None
+        self.last_alpha = None
+        self.last_projection = None
+        self._work = None
+        desvars = problem.get_desvars()
+        dg = problem.nabla_g()
+        problem.set_desvars(self.project_to_feasible(desvars.clone(), desvars, dg))
+
+    def _ws(self, n):
+        lib = _lib.load()
+        need = int(lib.pf_pgd_workspace_size(n))
+        if self._work is None or self._work.numel() < need:
+            self._work = torch.empty(need, dtype=torch.float64, device=device())
+        return self._work
+
+    def _stats(self, desvars, df, history):
+        n = desvars.shape[0]
+        out = (ctypes.c_double * 8)()
+        xl = self.last_desvars if history else None
+        dfl = self.last_nabla_f if history else None
+        _lib.check(_lib.load().pf_pgd_stats_f64(n, _lib.ptr(desvars), _lib.ptr(df), _lib.ptr(xl), _lib.ptr(dfl),
+                                                _lib.ptr(self._ws(n)), out, _lib.stream()))
+        return list(out)
+
+    @staticmethod
+    def _nan_to_num(v):
+        if math.isnan(v):
+            return 0.0
+        if math.isinf(v):
+            return sys.float_info.max if v > 0 else -sys.float_info.max
+        return v
+
+    def alpha(self, desvars, df):
+        """(alpha, beta): the step size and the conjugate-direction weight (None: d = -df)."""
+        hist = self.iteration > 0
+        dfdf, dfmax, dfdl, dldl, sy, ss, yy, ymax = self._stats(desvars, df, hist)
+        beta = None
+        if self.conjugate and self.iteration > 0:
+            # dx_n = -df, dx_n-1 = -df_last: dx_n.(dx_n - dx_n-1) = df.df - df.df_last
+            beta = max((dfdf - dfdl) / dldl, 0.0)
+        if self.iteration == 0:
+            alpha = self.fall_back_move / dfmax
+        elif float(self.problem.g().max()) > self.tol_N and self.iteration > self.warmup_iter:
+            alpha = self.fall_back_move / dfmax
+        else:
+            if sy > 1e-6:
+                alpha = ss / sy
+                L = self._nan_to_num(math.sqrt(yy) / math.sqrt(ss) if ss > 0 else (math.nan if yy == 0 else math.inf))
+                alpha = min(max(alpha, 1e-6), min(2 * self.relaxation / (L + 1e-6), self.alpha_max))
+            else:
+                if ymax <= 1e-8:  # np.allclose(y, 0): perfect linear behaviour
+                    L = math.sqrt(dfdf) * (math.sqrt(ss) / math.sqrt(self.problem.N()))
+                    alpha = self.relaxation / (L + 1e-6)
+                else:
+                    L = self._nan_to_num(math.sqrt(yy) / math.sqrt(ss) if ss > 0 else math.inf)
+                    alpha = min(self.relaxation / (L + 1e-6), self.alpha_max)
+        return alpha, beta
+
+    def project_to_feasible(self, desvars_new, desvars, dg):
+        n = desvars_new.shape[0]
+        out = (ctypes.c_double * 3)()
+        x_new = torch.empty_like(desvars_new)
+        desvars_new, dg = desvars_new.contiguous(), dg.contiguous()
+        _lib.check(_lib.load().pf_pgd_project_f64(n, _lib.ptr(desvars_new), _lib.ptr(dg),
+                                                  float(self.problem.volume_fraction), float(self.bounds[0]),
+                                                  float(self.bounds[1]), float(self.tol_B), _lib.ptr(x_new),
+                                                  _lib.ptr(self._ws(n)), out, _lib.stream()))
+        self.last_projection = {"l": out[0], "steps": int(out[1]), "feasible_at_zero": bool(out[2])}
+        return x_new
+
+    def iter(self):
+        if self.timer:
+            start = time.time()
+        p = self.problem
+        desvars = p.get_desvars()
+        dg = p.nabla_g()
+        df = p.nabla_f().clone()
+        f = p.f()
+        alpha, beta = self.alpha(desvars, df)
+        n = desvars.shape[0]
+        d = torch.empty_like(desvars)
+        x_step = torch.empty_like(desvars)
+        d_last = self.d_last if beta is not None else None
+        _lib.check(_lib.load().pf_pgd_step_f64(n, _lib.ptr(desvars), _lib.ptr(df), _lib.ptr(d_last),
+                                               float(beta if beta is not None else 0.0), float(alpha), _lib.ptr(d),
+                                               _lib.ptr(x_step), _lib.stream()))
+        self.last_alpha = alpha
+        self.last_nabla_f = df
+        self.d_last = d
+        self.last_desvars = desvars.clone()
+        self.last_f = f
+        self.iteration += 1
+        desvars_new = self.project_to_feasible(x_step, desvars, dg)
+        if self.timer:
+            end = time.time()
+        p.set_desvars(desvars_new)
+        self.change = float(torch.linalg.norm(self.last_desvars - desvars_new))
+        fn = p.f()
+        self.change_f = float(abs((fn - self.last_f) / fn))
         if self.timer:
             return end - start
 

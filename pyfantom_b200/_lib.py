@@ -97,6 +97,10 @@ SIGNATURES = {
     "pf_oc_workspace_size": (_SZ, [_LL]),
     "pf_oc_update_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
     "pf_oc_update_noalloc_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "pf_pgd_workspace_size": (_SZ, [_LL]),
+    "pf_pgd_stats_f64": (_I, [_LL, _P, _P, _P, _P, _P, _P, _P]),
+    "pf_pgd_step_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "pf_pgd_project_f64": (_I, [_LL, _P, _P, _D, _D, _D, _D, _P, _P, _P, _P]),
     "pf_cnn_conv3d_fwd_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P]),
     "pf_cnn_conv3d_bwd_data_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P]),
     "pf_cnn_conv3d_bwd_weight_workspace": (_SZ, [_I, _I]),

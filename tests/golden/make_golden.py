@@ -294,6 +294,53 @@ def mbb_trajectory():
     return f
 
 
+def pgd_goldens():
+    """PGD (reference defaults, conjugate directions) on the config-1 MBB half-beam for 30
+    iterations with the direct solver, the step size it chose at every iteration, and the
+    reference's projection onto the volume constraint on stand-alone cases."""
+    from pyFANTOM.Optimizers.CPU.PGD import PGD
+    wl = workloads.mbb2d(120, 40)
+    _, _, fe, prob = _simp_setup(wl, lambda m, k: SPSOLVE(k), 1.5, 0.5)
+    t = time.time()
+    x0 = np.array(prob.get_desvars())
+    pgd = PGD(prob)
+    out = {"x0": x0, "x_init": np.array(prob.get_desvars())}
+    alphas = []
+    orig = pgd.alpha
+
+    def rec(*a):
+        r = orig(*a)
+        alphas.append(float(r[0]))
+        return r
+
+    pgd.alpha = rec
+    f, change, change_f = [], [], []
+    for it in range(30):
+        pgd.iter()
+        f.append(float(pgd.last_f))
+        change.append(float(pgd.change))
+        change_f.append(float(pgd.change_f))
+        if it in (0, 1, 9, 29):
+            out[f"x{it + 1}"] = np.array(prob.get_desvars())
+    out.update(f=np.array(f), change=np.array(change), change_f=np.array(change_f), alpha=np.array(alphas),
+               f_final=np.array(float(prob.f())))
+    print(f"pgd: {time.time() - t:.1f}s f1={f[0]!r} f30={f[-1]!r}")
+    # stand-alone projections: x_new = clip(xs + l dg, 0, 1) with the bisected l
+    rng = np.random.default_rng(13)
+    for tag, n, vf, lo, hi in [("p1", 4000, 0.4, -0.3, 1.4), ("p2", 2500, 0.25, 0.0, 1.0), ("p3", 3000, 0.6, -0.1, 0.5)]:
+        xs = rng.uniform(lo, hi, n)
+        dg = np.full(n, 1.0 / n)
+        fake = _FixedProblem(np.clip(xs, 0, 1), np.zeros(n), vf)
+        fake.dg = dg
+        q = PGD.__new__(PGD)
+        q.problem, q.is_independent, q.m, q.bounds, q.tol_B = fake, True, 1, (0, 1.0), 1e-8
+        out[f"{tag}_xs"] = xs
+        out[f"{tag}_vf"] = np.array(vf)
+        out[f"{tag}_xnew"] = np.array(q.project_to_feasible(xs.copy(), xs.copy(), dg))
+    save("pgd", **out)
+    return f
+
+
 def sensitivity_goldens():
     """Compliance and its filtered sensitivity on a small bridge (direct solve)."""
     wl = workloads.bridge3d(12, 6, 6, seed=3)
@@ -339,7 +386,11 @@ def big_solve():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--big", action="store_true")
+    ap.add_argument("--only", default=None, help="run one generator (e.g. pgd)")
     args = ap.parse_args()
+    if args.only:
+        globals()[f"{args.only}_goldens"]()
+        return
     k0_goldens()
     operator_goldens()
     transfer_goldens()
@@ -349,6 +400,7 @@ def main():
     sensitivity_goldens()
     solve_goldens()
     f = mbb_trajectory()
+    pgd_goldens()
     ka_path = os.path.join(HERE, "known_answers.json")
     ka = json.load(open(ka_path)) if os.path.exists(ka_path) else {}
     ka["mbb_120x40"] = {"f_init": f[0], "f_iter1": f[1], "f_iter50": f[50]}

@@ -162,3 +162,23 @@ def test_workloads():
     assert b["fixed_dofs"].size == 2 * 5 * 3
     m = workloads.mbb2d(12, 4)
     assert m["fixed_dofs"].size == 5 + 1
+
+
+@pytest.mark.parametrize("tag", ["p1", "p2", "p3"])
+def test_pgd_projection_matches_reference(golden, tag):
+    g = golden("pgd")
+    xs = g[tag + "_xs"]
+    x, l, steps = O.pgd_project(xs, np.full(xs.size, 1.0 / xs.size), float(g[tag + "_vf"]))
+    assert np.array_equal(x, g[tag + "_xnew"]) or rel(x, g[tag + "_xnew"]) < 1e-14
+    if tag == "p3":  # clip(xs) already satisfies the constraint: no shift
+        assert steps == 0 and l == 0.0
+    else:
+        assert steps > 20 and l < 0
+
+
+def test_pgd_golden_trajectory_sane(golden):
+    g = golden("pgd")
+    f = g["f"]
+    assert f[0] == pytest.approx(1026.843067509509, rel=1e-13) and f[-1] < 0.25 * f[0]
+    assert g["alpha"].shape == (30,) and np.all(g["alpha"] > 0)
+    assert abs(g["x_init"].mean() - 0.5) < 1e-12
