@@ -78,7 +78,9 @@ def test_pgd_trajectory_matches_reference(golden):
     g = golden("pgd")
     wl, prob, fe = _mbb_problem()
     pgd = PGD(prob)  # initialises the design (uniform volume fraction) and projects it
-    assert rel(prob.get_desvars().cpu().numpy(), g["x_init"]) < 1e-15
+    # the uniform design sits on the constraint: the reference's sum came out a rounding
+    # error above the volume fraction (a shift of 2e-15), this one exactly on it
+    assert rel(prob.get_desvars().cpu().numpy(), g["x_init"]) < 1e-12
     f, alpha, change = [], [], []
     for it in range(30):
         pgd.iter()
