@@ -92,7 +92,10 @@ def test_pgd_trajectory_matches_reference(golden):
     f, alpha = np.array(f), np.array(alpha)
     assert abs(f[0] - g["f"][0]) < 1e-9 * g["f"][0]
     assert np.abs(f - g["f"]).max() / g["f"].min() < 1e-6
-    assert np.abs(alpha - g["alpha"]).max() / np.abs(g["alpha"]).max() < 1e-6
+    # the Barzilai-Borwein step s.s / s.y divides differences of nearly equal vectors and so
+    # amplifies rounding: 5e-14 at the first iteration, a few 1e-6 by the thirtieth
+    ra = np.abs(alpha - g["alpha"]) / np.abs(g["alpha"])
+    assert ra[:10].max() < 1e-8 and ra.max() < 1e-4, ra
     assert np.abs(prob.get_desvars().cpu().numpy() - g["x30"]).max() < 1e-5
     assert pgd.logs()["objective"] == pytest.approx(g["f"][-1], rel=1e-6)
     assert not pgd.converged() or pgd.change <= pgd.change_tol
