@@ -92,10 +92,11 @@ def test_pgd_trajectory_matches_reference(golden):
     f, alpha = np.array(f), np.array(alpha)
     assert abs(f[0] - g["f"][0]) < 1e-9 * g["f"][0]
     assert np.abs(f - g["f"]).max() / g["f"].min() < 1e-6
-    # the Barzilai-Borwein step s.s / s.y divides differences of nearly equal vectors and so
-    # amplifies rounding: 5e-14 at the first iteration, a few 1e-6 by the thirtieth
+    # the solves differ at their 1e-11 tolerance (MGCG here, a direct solve in the reference),
+    # and the Barzilai-Borwein step s.s / s.y divides differences of nearly equal vectors, so
+    # step sizes agree to 2e-11 at the first iteration, 3e-8 at the tenth, 6e-6 at worst
     ra = np.abs(alpha - g["alpha"]) / np.abs(g["alpha"])
-    assert ra[:10].max() < 1e-8 and ra.max() < 1e-4, ra
+    assert ra[0] < 1e-9 and ra[:10].max() < 1e-6 and ra.max() < 1e-4, ra
     assert np.abs(prob.get_desvars().cpu().numpy() - g["x30"]).max() < 1e-5
     assert pgd.logs()["objective"] == pytest.approx(g["f"][-1], rel=1e-6)
     assert not pgd.converged() or pgd.change <= pgd.change_tol
