@@ -248,6 +248,19 @@ size_t pf_cnn_energy_loss_workspace(void);
 int pf_cnn_energy_loss_f64(long long n, const double* y, const double* Ky, const double* b, double c, float* grad,
                            double* loss, double* work, void* stream);
 
+/* ---- multi-material SIMP (pyFANTOM/Problem/CUDA/MinimumCompliance.py:326-349,369-411) */
+/* E[e] = max(sum_i E_mul_i a_i prod_{j!=i} (1 - a_j), void), a_i = H(rho_i)^p, and
+ * dE[k][e] = dE/drho_k; rho and dE material-major [nm][ne]; 2 <= nm <= 8; h_E_mul host. */
+int pf_penalize_multi_f64(long long ne, int nm, const double* rho, const pf_simp_params* p, const double* h_E_mul,
+                          double* E, double* dE, void* stream);
+/* OC with one volume constraint per material (variables material-major, dg the per-variable
+ * constraint gradient, h_vf host [nm]): the multipliers are bisected in lockstep until all
+ * meet the stopping rule (Optimizers/CUDA/OC.py:104-127).  h_out as pf_oc_update_f64
+ * (lambda and steps of material 0). */
+size_t pf_oc_multi_workspace_size(long long ne, int nm);
+int pf_oc_update_multi_f64(long long ne, int nm, const double* x, const double* df, const double* dg,
+                           const double* h_vf, double move, double* x_new, double* work, double* h_out, void* stream);
+
 /* ---- PGD (pyFANTOM/Optimizers/CUDA/PGD.py:6-372), single volume constraint ---------- */
 size_t pf_pgd_workspace_size(long long n); /* doubles, for both calls below */
 /* h_out[8] (host) = {df.df, max|df|, df.df_last, df_last.df_last, s.y, s.s, y.y, max|y|}

@@ -306,6 +306,40 @@ def oc_update(x, df, dg, vf, move):
     return out, int(steps)
 
 
+def penalize_multi(rho, E_mul, penalty=3.0, void=1e-9, heavyside=False, beta=2.0, eta=0.5):
+    """Multi-material SIMP law and its gradient (pyFANTOM/Problem/CPU/MinimumCompliance.py
+    multi-material branches): rho [nel, nm] -> (E [nel], dE [nel, nm]) with a_i = H(rho_i)^p,
+    E = max(sum_i E_mul_i a_i prod_{j != i} (1 - a_j), void) and its derivative."""
+    rho = np.asarray(rho, np.float64)
+    E_mul = np.asarray(E_mul, np.float64)
+    nm = rho.shape[1]
+    if heavyside:
+        den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+        h = (np.tanh(beta * eta) + np.tanh(beta * (rho - eta))) / den
+        dh = beta * (1 - np.tanh(beta * (rho - eta)) ** 2) / den
+    else:
+        h, dh = rho, np.ones_like(rho)
+    a, da = h ** penalty, penalty * h ** (penalty - 1)
+    b = 1.0 - a
+    E = np.zeros(rho.shape[0])
+    dE = np.zeros_like(rho)
+    for i in range(nm):
+        t = a[:, i].copy()
+        for j in range(nm):
+            if j != i:
+                t *= b[:, j]
+        E += E_mul[i] * t
+    for k in range(nm):
+        for i in range(nm):
+            t = da[:, k].copy() if i == k else -da[:, k] * a[:, i]
+            for j in range(nm):
+                if j != i and j != k:
+                    t *= b[:, j]
+            dE[:, k] += E_mul[i] * t
+        dE[:, k] *= dh[:, k]
+    return np.maximum(E, void), dE
+
+
 def pgd_project(xs, dg, vf, lo=0.0, hi=1.0, tol=1e-8):
     """The reference PGD projection for one volume constraint
     (pyFANTOM/Optimizers/CPU/PGD.py:144-170): clip(xs + l dg, lo, hi) with l bisected in

@@ -4,7 +4,9 @@ Optimizers/_optimizer.py).
 ``OC.iter()`` computes ``ocP = x sqrt(max(-df/dg, 0))`` and bisects the Lagrange
 multiplier with the reference's initial bracket [1e-9, 1e9], midpoint rule and stopping
 test ``(l2-l1)/(l2+l1) <= 1e-8``; the bisection runs on the device (``pf_oc_update_f64``,
-five bisection levels per sweep over the elements, no host round trip per step).
+five bisection levels per sweep over the elements, no host round trip per step).  With
+one volume constraint per material the multipliers are bisected in lockstep as in the
+reference (``pf_oc_update_multi_f64``).
 ``converged()`` and ``logs()`` keep the reference keys.
 """
 from __future__ import annotations
@@ -41,8 +43,6 @@ class OC(Optimizer):
         super().__init__(problem)
         if not problem.is_independent():
             raise ValueError("OC optimizer requires a problem with independent constraints.")
-        if problem.m() != 1:
-            raise NotImplementedError("OC here supports a single volume constraint")
         self.last_desvars = problem.get_desvars().clone()
         self.last_f = problem.f()
         self.m = problem.m()
@@ -59,7 +59,26 @@ class OC(Optimizer):
         self.last_lambda = None
         self.last_steps = None
 
+    def _oc_step_multi(self, x, df, dg, vf):
+        nm = self.m
+        ne = x.shape[0] // nm
+        lib = _lib.load()
+        need = int(lib.pf_oc_multi_workspace_size(ne, nm))
+        if self._work is None or self._work.numel() < need:
+            self._work = torch.empty(need, dtype=torch.float64, device=device())
+        x_new = torch.empty_like(x)
+        out = (ctypes.c_double * 3)()
+        dgs = dg.sum(dim=0).contiguous()  # per-variable constraint gradient (OC.py:69-70)
+        df = df.contiguous()
+        vf_h = (ctypes.c_double * nm)(*[float(v) for v in vf])
+        _lib.check(lib.pf_oc_update_multi_f64(ne, nm, _lib.ptr(x), _lib.ptr(df), _lib.ptr(dgs), vf_h,
+                                              float(self.move), _lib.ptr(x_new), _lib.ptr(self._work), out,
+                                              _lib.stream()))
+        return x_new, out[0], out[1], int(out[2])
+
     def _oc_step(self, x, df, dg, vf):
+        if self.m > 1:
+            return self._oc_step_multi(x, df, dg, vf)
         n = x.shape[0]
         lib = _lib.load()
         if self._work is None or self._work.numel() < lib.pf_oc_workspace_size(n):
@@ -77,7 +96,7 @@ class OC(Optimizer):
             start = time.time()
         p = self.problem
         x = p.get_desvars()
-        vf = p.volume_fraction
+        vf = p.volume_fraction if p.is_single_material else p._vf_h
         x_new, change, lam, steps = self._oc_step(x, p.nabla_f(), p.nabla_g(), vf)
         self.last_lambda, self.last_steps = lam, steps
         self.iteration += 1

@@ -30,6 +30,8 @@ __all__ = ["compliance", "volume", "Compliance", "Volume"]
 class Compliance(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, problem):
+        if not problem.is_single_material:
+            raise NotImplementedError("the differentiable compliance covers single-material problems")
         x = as_cuda(x.detach(), torch.float64)
         rho = problem.filter.dot(x)
         E = problem.penalize(rho)

@@ -13,6 +13,8 @@
 // exactly as the sequential loop forms them, so the sequence of (l1, l2) is the same.
 #include <cmath>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace pf {
@@ -37,6 +39,52 @@ __global__ void k_penalize(long long n, const double* __restrict__ rho, pf_simp_
             E[i] = fmax(e, P.void_value);
         }
         if (dE) dE[i] = P.penalty * pow(r, P.penalty - 1.0) * dh * P.E_mul;
+    }
+}
+
+// Multi-material SIMP (pyFANTOM/Problem/CUDA/MinimumCompliance.py:326-349, 369-411): with
+// a_i = H(rho_i)^p and b_i = 1 - a_i,
+//   E = max(sum_i E_mul_i a_i prod_{j != i} b_j, void)
+//   dE/drho_k = H'(rho_k) sum_i E_mul_i { p H^(p-1)(rho_k) prod_{j != k} b_j            (i = k)
+//                                         -p H^(p-1)(rho_k) a_i prod_{j != i, k} b_j     (i != k) }
+// rho and dE are material-major [n_material][n_elements] (the design-variable order).
+constexpr int kMaxMaterials = 8;
+struct MultiEmul {
+    double v[kMaxMaterials];
+};
+__global__ void k_penalize_multi(long long ne, int nm, const double* __restrict__ rho, pf_simp_params P, MultiEmul em,
+                                 double* __restrict__ E, double* __restrict__ dE) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += (long long)gridDim.x * blockDim.x) {
+        double a[kMaxMaterials], b[kMaxMaterials], da[kMaxMaterials];
+        for (int k = 0; k < nm; k++) {
+            double r = rho[k * ne + e], dh = 1.0;
+            if (P.heavyside) heavy(rho[k * ne + e], P.beta, P.eta, &r, &dh);
+            a[k] = pow(r, P.penalty);
+            b[k] = 1.0 - a[k];
+            da[k] = P.penalty * pow(r, P.penalty - 1.0) * dh;
+        }
+        if (E) {
+            double s = 0.0;
+            for (int i = 0; i < nm; i++) {
+                double t = a[i];
+                for (int j = 0; j < nm; j++)
+                    if (j != i) t *= b[j];
+                s += em.v[i] * t;
+            }
+            E[e] = fmax(s, P.void_value);
+        }
+        if (dE) {
+            for (int k = 0; k < nm; k++) {
+                double s = 0.0;
+                for (int i = 0; i < nm; i++) {
+                    double t = i == k ? da[k] : -da[k] * a[i];
+                    for (int j = 0; j < nm; j++)
+                        if (j != i && j != k) t *= b[j];
+                    s += em.v[i] * t;
+                }
+                dE[k * ne + e] = s;
+            }
+        }
     }
 }
 
@@ -232,6 +280,81 @@ __global__ void __launch_bounds__(kRT) k_oc_change(const double* partials, int n
     if (threadIdx.x == 0) S->change2 = s;
 }
 
+// Several volume constraints (one per material, variables material-major): the reference
+// bisects all multipliers in lockstep while any of them is unconverged (OC.py:111-127),
+// so every multiplier takes the same number of steps.  One OcState per material; the
+// evaluation pass runs per material segment, this kernel replays the lockstep decisions.
+struct MultiVf {
+    double v[kMaxMaterials];
+};
+__global__ void __launch_bounds__(32) k_oc_step_multi(const double* partials, int np, int nm, MultiVf vf, OcState* S) {
+    if (S[0].done) return;
+    const int t = threadIdx.x;
+    for (int k = 0; k < nm; k++) {
+        if (t < kOcTree) {
+            double s = 0.0;
+            const double* pk = partials + (size_t)k * np * kOcTree;
+            for (int b = 0; b < np; b++) s += pk[(long long)b * kOcTree + t];
+            S[k].g[t] = s - vf.v[k];
+        }
+    }
+    __syncwarp();
+    if (t == 0) {
+        int node[kMaxMaterials];
+        for (int k = 0; k < nm; k++) node[k] = 0;
+        bool done = false;
+        for (int d = 0; d < 5 && !done; d++) {
+            bool any = false;
+            for (int k = 0; k < nm; k++) any |= (S[k].l2 - S[k].l1) / (S[k].l2 + S[k].l1) > 1e-8;
+            if (!any) {
+                done = true;
+                break;
+            }
+            for (int k = 0; k < nm; k++) {
+                const double lmid = S[k].lam[node[k]];
+                S[k].lmid = lmid;
+                S[k].steps += 1;
+                if (S[k].g[node[k]] <= 0.0) {
+                    S[k].l2 = lmid;
+                    node[k] = 2 * node[k] + 1;
+                } else {
+                    S[k].l1 = lmid;
+                    node[k] = 2 * node[k] + 2;
+                }
+            }
+        }
+        if (!done) {
+            bool any = false;
+            for (int k = 0; k < nm; k++) any |= (S[k].l2 - S[k].l1) / (S[k].l2 + S[k].l1) > 1e-8;
+            done = !any;
+        }
+        for (int k = 0; k < nm; k++) {
+            S[k].done = done;
+            if (!done) oc_tree(&S[k]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kRT) k_oc_init_multi(const double* partials, int np, int nm, OcState* S) {
+    __shared__ double s_red[kRT / 32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+    s = block_sum<kRT>(s, s_red);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < nm; k++) {
+            S[k].abs_sum = s;
+            S[k].allzero = s == 0.0;
+            S[k].l1 = 1e-9;
+            S[k].l2 = 1e9;
+            S[k].lmid = 0.0;
+            S[k].done = 0;
+            S[k].steps = 0;
+            S[k].change2 = 0.0;
+            oc_tree(&S[k]);
+        }
+    }
+}
+
 static unsigned oc_blocks(long long n) {
     long long nb = (n + kRT - 1) / kRT;
     if (nb > 2LL * kNumSM) nb = 2LL * kNumSM;
@@ -275,9 +398,82 @@ int oc_update(long long n, const double* x, const double* df, const double* dg, 
     return PF_OK;
 }
 
+size_t oc_multi_workspace(long long ne, int nm) {
+    const long long n = ne * nm;
+    return (size_t)n + (size_t)oc_blocks(ne) * kOcTree * nm + (size_t)oc_blocks(n) +
+           (sizeof(OcState) * nm + 7) / 8 + 8;
+}
+
+int oc_update_multi(long long ne, int nm, const double* x, const double* df, const double* dg, const double* vf,
+                    double move, double* x_new, double* work, double* h_out, cudaStream_t st) {
+    const long long n = ne * nm;
+    const unsigned nb = oc_blocks(ne), nbn = oc_blocks(n);
+    double* ocp = work;
+    double* partials = work + n;                               // nm segments of nb * kOcTree
+    double* sums = partials + (size_t)nb * kOcTree * nm;        // nbn
+    OcState* S = reinterpret_cast<OcState*>(sums + nbn);
+    MultiVf mv;
+    for (int k = 0; k < nm; k++) mv.v[k] = vf[k];
+    pf::count_launch(2);
+    k_oc_prep<<<nbn, kRT, 0, st>>>(n, x, df, dg, ocp, sums);
+    k_oc_init_multi<<<1, kRT, 0, st>>>(sums, nbn, nm, S);
+    for (int p = 0; p < kOcPasses; p++) {
+        for (int k = 0; k < nm; k++) {
+            pf::count_launch();
+            k_oc_eval<<<nb, kRT, 0, st>>>(ne, x + k * ne, ocp + k * ne, dg + k * ne, move, &S[k],
+                                          partials + (size_t)k * nb * kOcTree);
+        }
+        pf::count_launch();
+        k_oc_step_multi<<<1, 32, 0, st>>>(partials, nb, nm, mv, S);
+    }
+    for (int k = 0; k < nm; k++) {
+        pf::count_launch();
+        k_oc_write<<<nb, kRT, 0, st>>>(ne, x + k * ne, ocp + k * ne, move, &S[k], x_new + k * ne,
+                                       partials + (size_t)k * nb * kOcTree);
+    }
+    PF_LAUNCH_CHECK("oc multi launch");
+    if (h_out) {  // change^2: the per-block sums k_oc_write left in each material's segment
+        std::vector<OcState> h(nm);
+        std::vector<double> part((size_t)nb * kOcTree * nm);
+        PF_CUDA(cudaMemcpyAsync(h.data(), S, sizeof(OcState) * nm, cudaMemcpyDeviceToHost, st));
+        PF_CUDA(cudaMemcpyAsync(part.data(), partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st));
+        PF_CUDA(cudaStreamSynchronize(st));
+        double c2 = 0.0;
+        for (int k = 0; k < nm; k++)
+            for (unsigned b = 0; b < nb; b++) c2 += part[(size_t)k * nb * kOcTree + b];
+        h_out[0] = sqrt(c2);
+        h_out[1] = h[0].lmid;
+        h_out[2] = (double)h[0].steps;
+        if (!h[0].done) return fail(PF_NOT_CONVERGED, "OC bisection did not terminate in %d steps", h[0].steps);
+    }
+    return PF_OK;
+}
+
 }  // namespace pf
 
 using namespace pf;
+
+extern "C" int pf_penalize_multi_f64(long long ne, int nm, const double* rho, const pf_simp_params* p,
+                                     const double* h_E_mul, double* E, double* dE, void* stream) {
+    if (ne < 0 || nm < 2 || nm > kMaxMaterials || !rho || !p || !h_E_mul || (!E && !dE))
+        return fail(PF_BAD_ARG, "pf_penalize_multi_f64: bad argument (2..%d materials)", kMaxMaterials);
+    MultiEmul em;
+    for (int k = 0; k < nm; k++) em.v[k] = h_E_mul[k];
+    count_launch();
+    k_penalize_multi<<<grid_for(ne < 1 ? 1 : ne), kRT, 0, as_stream(stream)>>>(ne, nm, rho, *p, em, E, dE);
+    PF_LAUNCH_CHECK("penalize multi launch");
+    return PF_OK;
+}
+
+extern "C" size_t pf_oc_multi_workspace_size(long long ne, int nm) { return oc_multi_workspace(ne < 1 ? 1 : ne, nm); }
+
+extern "C" int pf_oc_update_multi_f64(long long ne, int nm, const double* x, const double* df, const double* dg,
+                                      const double* h_vf, double move, double* x_new, double* work, double* h_out,
+                                      void* stream) {
+    if (ne < 1 || nm < 1 || nm > kMaxMaterials || !x || !df || !dg || !h_vf || !x_new || !work)
+        return fail(PF_BAD_ARG, "pf_oc_update_multi_f64: bad argument (1..%d materials)", kMaxMaterials);
+    return oc_update_multi(ne, nm, x, df, dg, h_vf, move, x_new, work, h_out, as_stream(stream));
+}
 
 extern "C" int pf_penalize_f64(long long n, const double* rho, const pf_simp_params* p, double* E, double* dE,
                                void* stream) {

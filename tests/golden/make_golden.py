@@ -249,6 +249,43 @@ def penalize_goldens():
     save("penalize", **out)
 
 
+def multimaterial_goldens():
+    """Multi-material SIMP: penalize / penalize_grad for 2 and 3 materials (plain and
+    Heaviside), and 10 OC iterations of a 2-material MBB half-beam (48x16, direct solve)."""
+    mesh = StructuredMesh2D(4, 2, 4, 2, physics=LinearElasticity())
+    kern = StructuredStiffnessKernel(mesh)
+    fe = FiniteElement(mesh, kern, SPSOLVE(kern))
+    filt = StructuredFilter2D(mesh, 1.5)
+    rng = np.random.default_rng(17)
+    out = {}
+    for tag, nm, kw in [("m2", 2, dict(void=1e-9, penalty=3.0, heavyside=False)),
+                        ("m3", 3, dict(void=1e-9, penalty=3.0, heavyside=False)),
+                        ("m3h", 3, dict(void=1e-6, penalty=2.5, heavyside=True, beta=3.0, eta=0.45))]:
+        E_mul = [1.0, 0.6, 0.3][:nm]
+        prob = MinimumCompliance(fe, filt, E_mul=E_mul, volume_fraction=[0.2] * nm, **kw)
+        rho = rng.uniform(0.0, 1.0, (500, nm))
+        out[f"{tag}_rho"] = rho
+        out[f"{tag}_E"] = np.array(prob.penalize(rho))
+        out[f"{tag}_dE"] = np.array(prob.penalize_grad(rho))
+    wl = workloads.mbb2d(48, 16)
+    _, kern2, fe2, _ = _simp_setup(wl, lambda m, k: SPSOLVE(k), 1.5, 0.3)
+    filt2 = StructuredFilter2D(fe2.mesh, 1.5)
+    prob = MinimumCompliance(fe2, filt2, E_mul=[1.0, 0.5], void=1e-9, penalty=3.0, volume_fraction=[0.15, 0.15],
+                             heavyside=False)
+    oc = OC(prob, move=0.2)
+    out["mbb_x0"] = np.array(prob.get_desvars())
+    f = [float(prob.f())]
+    for _ in range(10):
+        oc.iter()
+        f.append(float(prob.f()))
+    out["mbb_f"] = np.array(f)
+    out["mbb_x10"] = np.array(prob.get_desvars())
+    out["mbb_df0"] = np.array(prob.nabla_f())
+    out["mbb_g10"] = np.array(prob.g())
+    print(f"multi-material mbb: f0={f[0]!r} f10={f[-1]!r}")
+    save("multimaterial", **out)
+
+
 def _simp_setup(wl, solver_factory, r_min, vf, void=1e-9, penalty=3.0):
     nel = wl["nel"]
     if wl["dim"] == 3:
@@ -401,6 +438,7 @@ def main():
     solve_goldens()
     f = mbb_trajectory()
     pgd_goldens()
+    multimaterial_goldens()
     ka_path = os.path.join(HERE, "known_answers.json")
     ka = json.load(open(ka_path)) if os.path.exists(ka_path) else {}
     ka["mbb_120x40"] = {"f_init": f[0], "f_iter1": f[1], "f_iter50": f[50]}

@@ -182,3 +182,14 @@ def test_pgd_golden_trajectory_sane(golden):
     assert f[0] == pytest.approx(1026.843067509509, rel=1e-13) and f[-1] < 0.25 * f[0]
     assert g["alpha"].shape == (30,) and np.all(g["alpha"] > 0)
     assert abs(g["x_init"].mean() - 0.5) < 1e-12
+
+
+@pytest.mark.parametrize("tag,kw", [("m2", dict(void=1e-9, penalty=3.0)), ("m3", dict(void=1e-9, penalty=3.0)),
+                                    ("m3h", dict(void=1e-6, penalty=2.5, heavyside=True, beta=3.0, eta=0.45))])
+def test_penalize_multi_matches_reference(golden, tag, kw):
+    g = golden("multimaterial")
+    rho = g[tag + "_rho"]
+    E_mul = [1.0, 0.6, 0.3][:rho.shape[1]]
+    E, dE = O.penalize_multi(rho, E_mul, **kw)
+    assert rel(E, g[tag + "_E"]) < 1e-14
+    assert rel(dE, g[tag + "_dE"]) < 1e-13
