@@ -141,7 +141,9 @@ class MinimumCompliance(Problem):
         if self.penalty_schedule is not None:
             pen = self.penalty_schedule(self.penalty, self.iteration)
         beta_val = self.beta(self.iteration) if callable(self.beta) else self.beta
-        return simp_params(pen, self.void, self.E_mul, beta_val, self.eta, self.heavyside)
+        # the multi-material kernel takes E_mul per material separately
+        emul = self.E_mul if self.is_single_material else 1.0
+        return simp_params(pen, self.void, emul, beta_val, self.eta, self.heavyside)
 
     def _penalize_multi(self, rho_mm, want_E=True, want_dE=True):
         """Material-major densities [n_material * nel] -> (E [nel], dE [n_material * nel])."""
