@@ -274,13 +274,14 @@ def multimaterial_goldens():
                              heavyside=False)
     oc = OC(prob, move=0.2)
     out["mbb_x0"] = np.array(prob.get_desvars())
+    out["mbb_df0"] = np.array(prob.nabla_f())
     f = [float(prob.f())]
     for _ in range(10):
         oc.iter()
         f.append(float(prob.f()))
     out["mbb_f"] = np.array(f)
     out["mbb_x10"] = np.array(prob.get_desvars())
-    out["mbb_df0"] = np.array(prob.nabla_f())
+    out["mbb_df10"] = np.array(prob.nabla_f())
     out["mbb_g10"] = np.array(prob.g())
     print(f"multi-material mbb: f0={f[0]!r} f10={f[-1]!r}")
     save("multimaterial", **out)

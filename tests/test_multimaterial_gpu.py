@@ -71,6 +71,8 @@ def test_two_material_oc_trajectory_matches_reference(golden):
     assert np.abs(f - g["mbb_f"]).max() / g["mbb_f"].min() < 1e-6
     assert np.abs(prob.get_desvars().cpu().numpy() - g["mbb_x10"]).max() < 1e-5
     assert np.abs(prob.g().cpu().numpy() - g["mbb_g10"]).max() < 1e-8
+    df10 = prob.nabla_f().cpu().numpy()
+    assert np.abs(df10 - g["mbb_df10"]).max() < 1e-5 * np.abs(g["mbb_df10"]).max()
     # thresholded re-solve of the mixture
     out = prob.FEA()
     assert float(out["compliance"]) > 0
