@@ -120,35 +120,38 @@ __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restric
     if (j0.x) j0.x[c * DIM + d] = (TO)((*j0.omega) * j0.scale) * j0.dinv[c * DIM + d] * bc;
 }
 
-// One thread per (fine node, component): P = Phat diag(1/tw), the mean of the 1, 2, 4 or 8
-// parent values divided by their tw.
+// One thread per fine node (all DIM components, contiguous loads of each parent): P =
+// Phat diag(1/tw), the mean of the 1, 2, 4 or 8 parent values divided by their tw.
 template <int DIM, typename T>
 __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict__ vc, T* __restrict__ vf,
                           const int* skip) {
     if (skip && *skip) return;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= gf.n_nodes * DIM) return;
-    const long long f = (unsigned)t / DIM;
-    const int d = (int)(t - f * DIM);
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= gf.n_nodes) return;
     int i, j, k;
     ndec(gf, f, i, j, k);
     const int i0 = i >> 1, j0 = j >> 1, k0 = DIM == 3 ? k >> 1 : 0;
     const int i1 = i0 + (i & 1), j1 = j0 + (j & 1), k1 = DIM == 3 ? k0 + (k & 1) : 0;
     auto itw = [&](int c, int n) { return (c == 0 || c == n - 1) ? T(1.0 / 1.5) : T(0.5); };
-    T acc = T(0);
+    T acc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) acc[d] = T(0);
     for (int cj = j0; cj <= j1; cj++) {
         const T wj = itw(cj, gc.nn[1]);
         for (int ci = i0; ci <= i1; ci++) {
             const T wij = wj * itw(ci, gc.nn[0]);
             for (int ck = k0; ck <= k1; ck++) {
                 const T w = DIM == 3 ? wij * itw(ck, gc.nn[2]) : wij;
-                acc += w * vc[nidx(gc, ci, cj, ck) * DIM + d];
+                const T* v = vc + nidx(gc, ci, cj, ck) * DIM;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) acc[d] += w * v[d];
             }
         }
     }
     const int nodd = (i & 1) + (j & 1) + (DIM == 3 ? (k & 1) : 0);
     const T scale = nodd == 0 ? T(1) : nodd == 1 ? T(0.5) : nodd == 2 ? T(0.25) : T(0.125);
-    vf[f * DIM + d] = acc * scale;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) vf[f * DIM + d] = acc[d] * scale;
 }
 
 template <typename TI, typename TO>
@@ -166,7 +169,7 @@ int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaS
 template <typename T>
 int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st) {
     const Grid gc = coarse_grid(gf);
-    const unsigned nb = (unsigned)((gf.n_nodes * gf.dim + 255) / 256);
+    const unsigned nb = (unsigned)((gf.n_nodes + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
         k_prolong<3, T><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vc, vf, skip);
