@@ -248,6 +248,18 @@ size_t pf_cnn_energy_loss_workspace(void);
 int pf_cnn_energy_loss_f64(long long n, const double* y, const double* Ky, const double* b, double c, float* grad,
                            double* loss, double* work, void* stream);
 
+/* ---- direct solve for small problems (the reference's SPSOLVE,
+ * solvers/CUDA/_solvers.py:245-328 with StructuredStiffnessKernel.construct,
+ * stiffness/CUDA/_FEA.py:484-516): dense assembly of the free-DOF block of K(E), tiled
+ * Cholesky and inverse factor, x = L^-T L^-1 b; constrained entries of x are b's.
+ * free_dofs [n_free] and dof_to_free [dof] (-1 when constrained) are int32 device
+ * arrays; n_free <= 20480. */
+typedef struct pf_direct pf_direct;
+int pf_direct_create(const pf_op* op, pf_direct** out);
+int pf_direct_destroy(pf_direct* d);
+int pf_direct_solve_f64(pf_direct* d, const double* E, const int* free_dofs, const int* dof_to_free, int n_free,
+                        const double* b, double* x, void* stream);
+
 /* ---- multi-material SIMP (pyFANTOM/Problem/CUDA/MinimumCompliance.py:326-349,369-411) */
 /* E[e] = max(sum_i E_mul_i a_i prod_{j!=i} (1 - a_j), void), a_i = H(rho_i)^p, and
  * dE[k][e] = dE/drho_k; rho and dE material-major [nm][ne]; 2 <= nm <= 8; h_E_mul host. */

@@ -97,6 +97,9 @@ SIGNATURES = {
     "pf_oc_workspace_size": (_SZ, [_LL]),
     "pf_oc_update_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
     "pf_oc_update_noalloc_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "pf_direct_create": (_I, [_P, ctypes.POINTER(_P)]),
+    "pf_direct_destroy": (_I, [_P]),
+    "pf_direct_solve_f64": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
     "pf_penalize_multi_f64": (_I, [_LL, _I, _P, ctypes.POINTER(pf_simp_params), _P, _P, _P, _P]),
     "pf_oc_multi_workspace_size": (_SZ, [_LL, _I]),
     "pf_oc_update_multi_f64": (_I, [_LL, _I, _P, _P, _P, _P, _D, _P, _P, _P, _P]),

@@ -179,7 +179,7 @@ void dense_free(Dense* d) {
     d->fail = nullptr;
 }
 
-int dense_factor_invert(Dense* d, double beta, cudaStream_t st) {
+int dense_factor_linv(Dense* d, double beta, cudaStream_t st) {
     const int np = d->np, nt = np / TB;
     PF_CUDA(cudaMemsetAsync(d->fail, 0, sizeof(int), st));
     pf::count_launch();
@@ -202,6 +202,14 @@ int dense_factor_invert(Dense* d, double beta, cudaStream_t st) {
         pf::count_launch();
         k_linv_row<<<i, dim3(TB, TB), 0, st>>>(d->M, d->Linv, np, i);
     }
+    PF_LAUNCH_CHECK("dense factorisation launch");
+    return PF_OK;
+}
+
+int dense_factor_invert(Dense* d, double beta, cudaStream_t st) {
+    int s = dense_factor_linv(d, beta, st);
+    if (s) return s;
+    const int np = d->np, nt = np / TB;
     pf::count_launch();
     k_ainv<<<dim3(nt, nt), dim3(TB, TB), 0, st>>>(d->Linv, d->Ainv, np, nt);
     PF_LAUNCH_CHECK("coarse factorisation launch");

@@ -51,6 +51,8 @@ int dense_alloc(Dense* d, int n);
 void dense_free(Dense* d);
 // M must hold the matrix (rows/cols >= n zero) before the call
 int dense_factor_invert(Dense* d, double beta, cudaStream_t st);
+// factor and inverse factor only (Linv = L^-1); no explicit inverse
+int dense_factor_linv(Dense* d, double beta, cudaStream_t st);
 template <typename T>
 int dense_solve(const Dense* d, const T* b, T* x, const int* skip, cudaStream_t st);
 

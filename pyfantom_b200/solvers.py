@@ -1,6 +1,9 @@
 """Linear solvers (drop-in for pyFANTOM/solvers/CUDA/_solvers.py and solvers/commons).
 
 * ``CG``        - matrix-free unpreconditioned CG (reference :22-132), ``pf_cg_solve``.
+* ``SPSOLVE``   - direct solve for small problems (reference :245-328): the free-DOF block
+  of K assembled dense on the device and factored by the library's tiled Cholesky
+  (``pf_direct_solve_f64``, up to 20,480 free DOFs).
 * ``MultiGrid`` - geometric-multigrid-preconditioned CG (reference :330-660) with the
   reference's V-cycle, damped-Jacobi smoother, adaptive omega schedule, Galerkin
   hierarchy and normalised transfers; the coarse solve is a dense Cholesky on the
@@ -25,7 +28,7 @@ import torch
 from . import _lib
 from ._tensor import as_cuda, device
 
-__all__ = ["Solver", "CG", "MultiGrid", "SolveInfo"]
+__all__ = ["Solver", "CG", "SPSOLVE", "MultiGrid", "SolveInfo"]
 
 logger = logging.getLogger(__name__)
 
@@ -89,6 +92,47 @@ class CG(Solver):
         r = rhs - k.dot(x)
         residual = float(torch.linalg.norm(r) / torch.linalg.norm(rhs))
         return x, residual
+
+
+class SPSOLVE(Solver):
+    """Direct solver (reference _solvers.py:245-328): solves the free DOFs of K(rho) exactly
+    (dense Cholesky on the device) and keeps the right-hand side on constrained DOFs."""
+
+    def __init__(self, kernel):
+        super().__init__()
+        if kernel.shape[0] > 3e6:
+            raise ValueError("Currently we do not allow spsolve for problem size bigger than 3M degrees of freedom.")
+        self.kernel = kernel
+        self.last_x0 = None
+        self._h = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib._lib.pf_direct_destroy(h)
+            self._h = None
+
+    def solve(self, rhs, rho=None, **kwargs):
+        k = self.kernel
+        if rho is not None:
+            k.set_rho(rho)
+        elif not k.has_rho:
+            raise ValueError("Solver requires a density vector to be passed or set on the kernel.")
+        lib = _lib.load()
+        if self._h is None:
+            h = ctypes.c_void_p()
+            _lib.check(lib.pf_direct_create(k._op, ctypes.byref(h)))
+            self._h = h
+        rhs = as_cuda(rhs, torch.float64)
+        free = torch.nonzero(~k.constraints).reshape(-1).to(torch.int32) if k.has_con else \
+            torch.arange(rhs.shape[0], dtype=torch.int32, device=device())
+        d2f = torch.full((rhs.shape[0],), -1, dtype=torch.int32, device=device())
+        d2f[free.long()] = torch.arange(free.numel(), dtype=torch.int32, device=device())
+        out = torch.empty_like(rhs)
+        _lib.check(lib.pf_direct_solve_f64(self._h, _lib.ptr(k.rho), _lib.ptr(free), _lib.ptr(d2f), int(free.numel()),
+                                           _lib.ptr(rhs), _lib.ptr(out), _lib.stream()))
+        residual = float(torch.linalg.norm(rhs - k.dot(out)) / torch.linalg.norm(rhs))
+        return out, residual
 
 
 class MultiGrid(Solver):
