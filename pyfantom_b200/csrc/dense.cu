@@ -148,6 +148,8 @@ __global__ void __launch_bounds__(1024) k_ainv(const double* Linv, double* Ainv,
 template <typename T>
 __global__ void __launch_bounds__(256) k_dense_matvec(const double* __restrict__ Ainv, int np, int n,
                                                       const T* __restrict__ b, T* __restrict__ x, const int* skip) {
+    pdl_wait();
+    pdl_trigger();
     if (skip && *skip) return;
     const int row = blockIdx.x * 8 + (threadIdx.x >> 5), l = threadIdx.x & 31;
     if (row >= n) return;
@@ -219,7 +221,8 @@ int dense_factor_invert(Dense* d, double beta, cudaStream_t st) {
 template <typename T>
 int dense_solve(const Dense* d, const T* b, T* x, const int* skip, cudaStream_t st) {
     pf::count_launch();
-    k_dense_matvec<T><<<(d->n + 7) / 8, 256, 0, st>>>(d->Ainv, d->np, d->n, b, x, skip);
+    PF_CUDA(launch_pdl(k_dense_matvec<T>, dim3((d->n + 7) / 8), dim3(256), 0, st, (const double*)d->Ainv, d->np, d->n, b,
+                       x, skip));
     PF_LAUNCH_CHECK("coarse solve launch");
     return PF_OK;
 }

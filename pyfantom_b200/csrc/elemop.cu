@@ -167,6 +167,8 @@ template <typename T, typename TE, int TY, int CM>
 __global__ void __launch_bounds__((TY + 1) * 32, 3)
     k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
                 const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int NW = TY + 1;
     constexpr int NT = NW * 32;
     constexpr int PR = TY + 2, PC = 33, NPE = PR * PC;
@@ -552,6 +554,8 @@ struct Q4K {
 template <typename T, typename TE>
 __global__ void __launch_bounds__(256) k_matvec_q4(int NX, int NY, const T* __restrict__ u, const TE* __restrict__ E,
                                                    const uint8_t* __restrict__ mask, const Q4K<T> K, Epi<T> epi) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[8];
     if (epi.skip && *epi.skip) return;
     const int nx = NX + 1, ny = NY + 1;
@@ -631,15 +635,15 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
         pf::count_launch();
         constexpr int CMS = sizeof(T) == 4 ? 1 : 2;  // the sparse variant of this precision
         if (cm != 0)
-            k_matvec_h8<T, TE, TY, CMS><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E,
-                                                                      mask, blk, cf, epi);
+            PF_CUDA(launch_pdl(k_matvec_h8<T, TE, TY, CMS>, dim3(grid), dim3((TY + 1) * 32), 0, st, g.nel[0], g.nel[1], g.nel[2], cx, u, E,
+                                                                      mask, blk, cf, epi));
         else
-            k_matvec_h8<T, TE, TY, 0><<<grid, (TY + 1) * 32, 0, st>>>(g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
-                                                                    blk, cf, epi);
+            PF_CUDA(launch_pdl(k_matvec_h8<T, TE, TY, 0>, dim3(grid), dim3((TY + 1) * 32), 0, st, g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
+                                                                    blk, cf, epi));
     } else {
         const long long nb = q4_num_blocks(g);
         pf::count_launch();
-        k_matvec_q4<T, TE><<<(unsigned)nb, 256, 0, st>>>(g.nel[0], g.nel[1], u, E, mask, make_q4k<T>(op), epi);
+        PF_CUDA(launch_pdl(k_matvec_q4<T, TE>, dim3((unsigned)nb), dim3(256), 0, st, g.nel[0], g.nel[1], u, E, mask, make_q4k<T>(op), epi));
     }
     PF_LAUNCH_CHECK("fine matvec launch");
     return PF_OK;

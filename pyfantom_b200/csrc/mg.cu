@@ -98,6 +98,8 @@ namespace pf {
 template <typename T>
 __global__ void k_jacobi0(long long n, const T* __restrict__ b, const T* __restrict__ dinv, const double* omega,
                           double scale, T* __restrict__ x, const int* skip) {
+    pdl_wait();
+    pdl_trigger();
     if (skip && *skip) return;
     const T w = (T)((*omega) * scale);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -111,6 +113,8 @@ __global__ void k_recip(long long n, T* v) {
 }
 
 __global__ void k_d2f_skip(long long n, const double* __restrict__ a, float* __restrict__ b, const int* skip) {
+    pdl_wait();
+    pdl_trigger();
     if (skip && *skip) return;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
@@ -121,6 +125,8 @@ template <typename TB>
 __global__ void __launch_bounds__(kRedThreads) k_dot_partial(long long n, const double* __restrict__ a,
                                                              const TB* __restrict__ b, double* partials,
                                                              const int* skip) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (skip && *skip) return;
     double s = 0.0;
@@ -137,6 +143,8 @@ __device__ double sum_partials(const double* partials, long long np, double* s_r
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_pcg_normb(const double* partials, long long np, PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     const double bb = sum_partials(partials, np, s_red);
     if (threadIdx.x == 0) {
@@ -157,6 +165,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_normb(const double* partial
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_pcg_rho0(const double* partials, long long np, PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double rz = sum_partials(partials, np, s_red);
@@ -170,6 +180,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_rho0(const double* partials
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_pcg_alpha(const double* partials, long long np, PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double pq = sum_partials(partials, np, s_red);
@@ -189,6 +201,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_alpha(const double* partial
 __global__ void __launch_bounds__(kRedThreads) k_pcg_xr(long long n, const double* __restrict__ p,
                                                         const double* __restrict__ q, double* __restrict__ x,
                                                         double* __restrict__ r, const PcgState* st, double* partials) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double a = st->alpha;
@@ -204,6 +218,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_xr(long long n, const doubl
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_pcg_check(const double* partials, long long np, PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double rr = sum_partials(partials, np, s_red);
@@ -228,6 +244,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_check(const double* partial
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_pcg_beta(const double* partials, long long np, PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double rz = sum_partials(partials, np, s_red);
@@ -244,6 +262,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_beta(const double* partials
 
 template <typename TZ>
 __global__ void k_pcg_p(long long n, const TZ* __restrict__ z, double* __restrict__ p, const PcgState* st, int init) {
+    pdl_wait();
+    pdl_trigger();
     if (st->done) return;
     const double b = st->beta;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -251,6 +271,8 @@ __global__ void k_pcg_p(long long n, const TZ* __restrict__ z, double* __restric
 }
 
 __global__ void k_f2d(long long n, const float* __restrict__ a, double* __restrict__ b) {
+    pdl_wait();
+    pdl_trigger();
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
 }
@@ -344,7 +366,7 @@ static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, 
     int s;
     if (!x_ready) {  // otherwise the restriction from the finer level did this sweep
         pf::count_launch();
-        k_jacobi0<T><<<vec_blocks(L.ndof), kRedThreads, 0, st>>>(L.ndof, b, dinv, omega, scale, X, skip);
+        PF_CUDA(launch_pdl(k_jacobi0<T>, dim3(vec_blocks(L.ndof)), dim3(kRedThreads), 0, st, L.ndof, b, dinv, omega, scale, X, skip));
         PF_LAUNCH_CHECK("jacobi0 launch");
     }
     for (int k = 1; k < mg->cfg.n_smooth; k++) {
@@ -597,6 +619,8 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
 // V-cycle (public) and PCG
 // ---------------------------------------------------------------------------------------
 __global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_omega, double d_omega, double omega) {
+    pdl_wait();
+    pdl_trigger();
     PcgState h;
     memset(&h, 0, sizeof(h));
     h.tol = tol;
@@ -611,7 +635,7 @@ __global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_o
 static int init_state(pf_mg* mg, double tol, int maxiter, double omega, cudaStream_t st) {
     const double min_omega = fmax(mg->cfg.omega / 2.0, mg->cfg.min_omega);
     pf::count_launch();
-    k_init_state<<<1, 1, 0, st>>>(mg->st, tol, maxiter, min_omega, mg->cfg.omega - min_omega, omega);
+    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, mg->st, tol, maxiter, min_omega, mg->cfg.omega - min_omega, omega));
     PF_LAUNCH_CHECK("state init");
     return PF_OK;
 }
@@ -625,11 +649,11 @@ extern "C" int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega,
     const long long n = mg->L[0].ndof;
     if (mg->fp32) {
         pf::count_launch();
-        k_d2f_skip<<<vec_blocks(n), kRedThreads, 0, st>>>(n, r, (float*)mg->L[0].b, nullptr);
+        PF_CUDA(launch_pdl(k_d2f_skip, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, r, (float*)mg->L[0].b, nullptr));
         float* res;
         if ((s = vcycle<float>(mg, 0, (const float*)mg->L[0].b, &res, nullptr, nullptr, st))) return s;
         pf::count_launch();
-        k_f2d<<<vec_blocks(n), kRedThreads, 0, st>>>(n, res, z);
+        PF_CUDA(launch_pdl(k_f2d, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, res, z));
     } else {
         double* res;
         if ((s = vcycle<double>(mg, 0, r, &res, nullptr, nullptr, st))) return s;
@@ -645,11 +669,11 @@ static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaSt
     int s;
     if (mg->fp32) {
         pf::count_launch();
-        k_d2f_skip<<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->r, (float*)mg->L[0].b, &mg->st->done);
+        PF_CUDA(launch_pdl(k_d2f_skip, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, (float*)mg->L[0].b, &mg->st->done));
         float* res;
         if ((s = vcycle<float>(mg, 0, (const float*)mg->L[0].b, &res, nullptr, nullptr, st))) return s;
         pf::count_launch();
-        k_dot_partial<float><<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->r, res, mg->partials, &mg->st->done);
+        PF_CUDA(launch_pdl(k_dot_partial<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, res, mg->partials, &mg->st->done));
         PF_LAUNCH_CHECK("dot launch");
         *z_out = res;
         *np_out = vec_blocks(n);
@@ -666,9 +690,9 @@ static int update_p(pf_mg* mg, const void* z, int init, cudaStream_t st) {
     const long long n = mg->L[0].ndof;
     pf::count_launch();
     if (mg->fp32)
-        k_pcg_p<float><<<vec_blocks(n), kRedThreads, 0, st>>>(n, (const float*)z, mg->p, mg->st, init);
+        PF_CUDA(launch_pdl(k_pcg_p<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const float*)z, mg->p, mg->st, init));
     else
-        k_pcg_p<double><<<vec_blocks(n), kRedThreads, 0, st>>>(n, (const double*)z, mg->p, mg->st, init);
+        PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)z, mg->p, mg->st, init));
     PF_LAUNCH_CHECK("p update launch");
     return PF_OK;
 }
@@ -684,17 +708,17 @@ static int pcg_iteration(pf_mg* mg, double* x, cudaStream_t st) {
     e.dot_of_y = 1;
     if ((s = fine_mv<double>(mg, mg->p, e, st))) return s;
     pf::count_launch();
-    k_pcg_alpha<<<1, kRedThreads, 0, st>>>(mg->partials, fine_matvec_num_blocks(mg->op, 0), mg->st);
+    PF_CUDA(launch_pdl(k_pcg_alpha, dim3(1), dim3(kRedThreads), 0, st, mg->partials, fine_matvec_num_blocks(mg->op, 0), mg->st));
     pf::count_launch();
-    k_pcg_xr<<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->p, mg->q, x, mg->r, mg->st, mg->partials);
+    PF_CUDA(launch_pdl(k_pcg_xr, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->p, mg->q, x, mg->r, mg->st, mg->partials));
     pf::count_launch();
-    k_pcg_check<<<1, kRedThreads, 0, st>>>(mg->partials, vec_blocks(n), mg->st);
+    PF_CUDA(launch_pdl(k_pcg_check, dim3(1), dim3(kRedThreads), 0, st, mg->partials, vec_blocks(n), mg->st));
     PF_LAUNCH_CHECK("pcg launch");
     const void* z;
     long long np;
     if ((s = precondition(mg, &z, &np, st))) return s;
     pf::count_launch();
-    k_pcg_beta<<<1, kRedThreads, 0, st>>>(mg->partials, np, mg->st);
+    PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st));
     PF_LAUNCH_CHECK("beta launch");
     return update_p(mg, z, 0, st);
 }
@@ -732,15 +756,15 @@ static int solve_start(pf_mg* mg, int use_x0, cudaStream_t st) {
         PF_CUDA(cudaMemcpyAsync(mg->r, mg->bi, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     pf::count_launch();
-    k_dot_partial<double><<<vec_blocks(n), kRedThreads, 0, st>>>(n, mg->bi, mg->bi, mg->partials, nullptr);
+    PF_CUDA(launch_pdl(k_dot_partial<double>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->bi, mg->bi, mg->partials, nullptr));
     pf::count_launch();
-    k_pcg_normb<<<1, kRedThreads, 0, st>>>(mg->partials, vec_blocks(n), mg->st);
+    PF_CUDA(launch_pdl(k_pcg_normb, dim3(1), dim3(kRedThreads), 0, st, mg->partials, vec_blocks(n), mg->st));
     PF_LAUNCH_CHECK("pcg start");
     const void* z;
     long long np;
     if ((s = precondition(mg, &z, &np, st))) return s;
     pf::count_launch();
-    k_pcg_rho0<<<1, kRedThreads, 0, st>>>(mg->partials, np, mg->st);
+    PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st));
     return update_p(mg, z, 1, st);
 }
 
@@ -868,7 +892,7 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
     PcgState* S = (PcgState*)(partials + npart);
     const int* skip = &S->done;
     pf::count_launch();
-    k_init_state<<<1, 1, 0, st>>>(S, tol, maxiter, 0.0, 0.0, 0.0);
+    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, S, tol, maxiter, 0.0, 0.0, 0.0));
     if (use_x0) {
         Epi<double> e = make_epi<double>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, r, nullptr, 1.0, nullptr);
         int s = launch_fine_matvec<double, double>(op, E, x, node_mask, e, st);
@@ -879,15 +903,15 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
     }
     const unsigned vb = vec_blocks(n);
     pf::count_launch();
-    k_dot_partial<double><<<vb, kRedThreads, 0, st>>>(n, b, b, partials, nullptr);
+    PF_CUDA(launch_pdl(k_dot_partial<double>, dim3(vb), dim3(kRedThreads), 0, st, n, b, b, partials, nullptr));
     pf::count_launch();
-    k_pcg_normb<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+    PF_CUDA(launch_pdl(k_pcg_normb, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
     pf::count_launch();
-    k_dot_partial<double><<<vb, kRedThreads, 0, st>>>(n, r, r, partials, skip);
+    PF_CUDA(launch_pdl(k_dot_partial<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, r, partials, skip));
     pf::count_launch();
-    k_pcg_rho0<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+    PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
     pf::count_launch();
-    k_pcg_p<double><<<vb, kRedThreads, 0, st>>>(n, r, p, S, 1);
+    PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, p, S, 1));
     PF_LAUNCH_CHECK("cg start");
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -906,15 +930,15 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
             int s = launch_fine_matvec<double, double>(op, E, p, node_mask, e, st);
             if (s) return s;
             pf::count_launch();
-            k_pcg_alpha<<<1, kRedThreads, 0, st>>>(partials, nbm, S);
+            PF_CUDA(launch_pdl(k_pcg_alpha, dim3(1), dim3(kRedThreads), 0, st, partials, nbm, S));
             pf::count_launch();
-            k_pcg_xr<<<vb, kRedThreads, 0, st>>>(n, p, q, x, r, S, partials);
+            PF_CUDA(launch_pdl(k_pcg_xr, dim3(vb), dim3(kRedThreads), 0, st, n, p, q, x, r, S, partials));
             pf::count_launch();
-            k_pcg_check<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+            PF_CUDA(launch_pdl(k_pcg_check, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
             pf::count_launch();
-            k_pcg_beta<<<1, kRedThreads, 0, st>>>(partials, vb, S);
+            PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
             pf::count_launch();
-            k_pcg_p<double><<<vb, kRedThreads, 0, st>>>(n, r, p, S, 0);
+            PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, p, S, 0));
         }
         PF_LAUNCH_CHECK("cg iteration");
         it += chunk;

@@ -78,6 +78,8 @@ static GridDev<DIM> gdev(const Grid& g) {
 template <int DIM, typename TI, typename TO>
 __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restrict__ vf, TO* __restrict__ vc,
                            const int* skip, Jacobi0<TO> j0) {
+    pdl_wait();
+    pdl_trigger();
     using TA = TO;  // accumulation precision
     if (skip && *skip) return;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -125,6 +127,8 @@ __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restric
 template <int DIM, typename T>
 __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict__ vc, T* __restrict__ vf,
                           const int* skip) {
+    pdl_wait();
+    pdl_trigger();
     if (skip && *skip) return;
     const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= gf.n_nodes) return;
@@ -160,9 +164,9 @@ int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaS
     const unsigned nb = (unsigned)((gc.n_nodes * gf.dim + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
-        k_restrict<3, TI, TO><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0);
+        PF_CUDA(launch_pdl(k_restrict<3, TI, TO>, dim3(nb), dim3(256), 0, st, gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0));
     else
-        k_restrict<2, TI, TO><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), vf, vc, skip, j0);
+        PF_CUDA(launch_pdl(k_restrict<2, TI, TO>, dim3(nb), dim3(256), 0, st, gdev<2>(gf), gdev<2>(gc), vf, vc, skip, j0));
     PF_LAUNCH_CHECK("restrict launch");
     return PF_OK;
 }
@@ -172,9 +176,9 @@ int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStre
     const unsigned nb = (unsigned)((gf.n_nodes + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
-        k_prolong<3, T><<<nb, 256, 0, st>>>(gdev<3>(gf), gdev<3>(gc), vc, vf, skip);
+        PF_CUDA(launch_pdl(k_prolong<3, T>, dim3(nb), dim3(256), 0, st, gdev<3>(gf), gdev<3>(gc), vc, vf, skip));
     else
-        k_prolong<2, T><<<nb, 256, 0, st>>>(gdev<2>(gf), gdev<2>(gc), vc, vf, skip);
+        PF_CUDA(launch_pdl(k_prolong<2, T>, dim3(nb), dim3(256), 0, st, gdev<2>(gf), gdev<2>(gc), vc, vf, skip));
     PF_LAUNCH_CHECK("prolong launch");
     return PF_OK;
 }
@@ -200,6 +204,8 @@ template int launch_prolong<float>(const Grid&, const float*, float*, const int*
 template <int DIM, typename T, bool HALF>
 __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
                                                                         const T* __restrict__ u, Epi<T> epi) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM, NG = NB / 3, C = NB / 2;
     __shared__ T s_part[NG][DIM][32];
     if (epi.skip && *epi.skip) return;
@@ -273,14 +279,14 @@ int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& e
     pf::count_launch();
     if (g.dim == 3) {
         if (half)
-            k_stencil_matvec<3, T, true><<<nb, 288, 0, st>>>(gdev<3>(g), A, u, epi);
+            PF_CUDA(launch_pdl(k_stencil_matvec<3, T, true>, dim3(nb), dim3(288), 0, st, gdev<3>(g), A, u, epi));
         else
-            k_stencil_matvec<3, T, false><<<nb, 288, 0, st>>>(gdev<3>(g), A, u, epi);
+            PF_CUDA(launch_pdl(k_stencil_matvec<3, T, false>, dim3(nb), dim3(288), 0, st, gdev<3>(g), A, u, epi));
     } else {
         if (half)
-            k_stencil_matvec<2, T, true><<<nb, 96, 0, st>>>(gdev<2>(g), A, u, epi);
+            PF_CUDA(launch_pdl(k_stencil_matvec<2, T, true>, dim3(nb), dim3(96), 0, st, gdev<2>(g), A, u, epi));
         else
-            k_stencil_matvec<2, T, false><<<nb, 96, 0, st>>>(gdev<2>(g), A, u, epi);
+            PF_CUDA(launch_pdl(k_stencil_matvec<2, T, false>, dim3(nb), dim3(96), 0, st, gdev<2>(g), A, u, epi));
     }
     PF_LAUNCH_CHECK("stencil matvec launch");
     return PF_OK;
