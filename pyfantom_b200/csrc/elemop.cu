@@ -523,9 +523,9 @@ static H8Blk<T> make_blk(const Op* op) {
 constexpr int kTY64 = 4;  // FP64: 5 warps per block
 constexpr int kTY32 = 8;  // FP32: 9 warps per block
 
-static void h8_launch_dims(const Grid& g, int TY, dim3* grid, int* CXc) {
+static void h8_launch_dims(const Grid& g, int TY, bool fp32, dim3* grid, int* CXc) {
     const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
-    const int zt = TY == kTY32 ? kZTile32 : kZTile64;
+    const int zt = fp32 ? kZTile32 : kZTile64;
     const int tz = (nz + zt - 1) / zt, ty = (ny + TY - 1) / TY;
     // enough x-chunks for ~4 waves of blocks, chunks of 4..32 planes
     const long long target = 4LL * kNumSM * 3;
@@ -539,7 +539,7 @@ static void h8_launch_dims(const Grid& g, int TY, dim3* grid, int* CXc) {
 long long h8_num_blocks(const Grid& g, int fp32) {
     dim3 gr;
     int cx;
-    h8_launch_dims(g, fp32 ? kTY32 : kTY64, &gr, &cx);
+    h8_launch_dims(g, fp32 ? kTY32 : kTY64, fp32 != 0, &gr, &cx);
     return (long long)gr.x * gr.y * gr.z;
 }
 
@@ -620,7 +620,7 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
         constexpr int TY = sizeof(T) == 8 ? kTY64 : kTY32;
         dim3 grid;
         int cx;
-        h8_launch_dims(g, TY, &grid, &cx);
+        h8_launch_dims(g, TY, sizeof(T) == 4, &grid, &cx);
         // FP32, isotropic box elements: the 33 nonzero coefficients (read as constant
         // operands); FP64: the 7 values of a cube element in registers, other boxes the
         // dense blocks from shared memory (33 double registers would cut the occupancy)
