@@ -402,6 +402,26 @@ def probe_matvec(args):
     return out
 
 
+def probe_solve(args):
+    """One cold solve of the workload after two warm-up solves, bracketed by
+    cudaProfilerStart/Stop (for `ncu --profile-from-start off`: the launch list of exactly
+    one solve, hierarchy setup included)."""
+    import torch
+    spec = WORKLOADS[args.workload]
+    wl, mesh, kern, sol, fe, E = build_problem(spec["nel"], spec["n_level"], args.precision)
+    kern.set_rho(E)
+    for _ in range(2):
+        sol.solve(fe.rhs, use_last=False)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    U, res = sol.solve(fe.rhs, use_last=False)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return {"probe": "solve", "workload": args.workload, "precision": args.precision,
+            "iterations": sol.last_info["iterations"], "status": sol.last_info["status"],
+            "solve_ms": sol.last_info["solve_ms"], "setup_ms": sol.last_info["setup_ms"]}
+
+
 # -----------------------------------------------------------------------------------------
 # reference arm and CPU baseline: the oracle (C/OpenMP restatement of the reference solve)
 # -----------------------------------------------------------------------------------------
@@ -451,7 +471,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--probe", choices=["matvec"], default=None,
+    ap.add_argument("--probe", choices=["matvec", "solve"], default=None,
                     help="only time the fine matvec (FP64 and FP32) at the workload size (for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
@@ -468,6 +488,9 @@ def main():
     import torch
     if args.probe == "matvec":
         print(json.dumps(probe_matvec(args)), flush=True)
+        return
+    if args.probe == "solve":
+        print(json.dumps(probe_solve(args)), flush=True)
         return
     if world > 1:
         import datetime
