@@ -163,7 +163,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // CM selects the element operator: 0 dense class blocks read from shared memory (any K0
 // with the reflection symmetry), 1 the 33 nonzeros of an isotropic box element, 2 the 7
 // values of a cube element (1, 2: coefficients held in registers).
-template <typename T, typename TE, int TY, int CM>
+template <typename T, typename TE, int TY, int CM, int MODE, bool DOT>
 __global__ void __launch_bounds__((TY + 1) * 32, 3)
     k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
                 const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
@@ -190,9 +190,10 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
     const bool owner = (w < TY) && (l < ZT) && (jn < ny) && (kn < nz);
     const bool col_ok = (l <= ZT) && (je >= 0) && (je < NY) && (ke >= 0) && (ke < NZ);
     const T wgt = epi_omega(epi);
-    const int mode = epi.mode;
-    const bool need_b = mode != PF_EPI_STORE, need_d = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
-    const bool need_xa = mode == PF_EPI_JACOBI_ADD, need_dot = epi.dot_partial != nullptr;
+    // the epilogue mode and the fused dot are compile-time: no per-step branches on them
+    constexpr int mode = MODE;
+    constexpr bool need_b = mode != PF_EPI_STORE, need_d = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
+    constexpr bool need_xa = mode == PF_EPI_JACOBI_ADD, need_dot = DOT;
     double dot = 0.0;
     constexpr int TB_ = (int)sizeof(T);
 
@@ -296,6 +297,8 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
     // held in 72 (FP32) / 144 (FP64) registers for the whole kernel
     const volatile T* vb = s_blk;
 #define BK(p, i, j) vb[(p) * 9 + (i) * 3 + (j)]
+    // cube element: diagonal minus off-diagonal of the two circulant class blocks
+    [[maybe_unused]] const T amb = cf.c[0] - cf.c[1], fmg = cf.c[5] - cf.c[6];
     // prologue: planes ix0-1 (buffer 0) and ix0 (buffer 1); FP32: plane ix0+1 in flight
     [[maybe_unused]] uint8_t mq[NQ];
     if constexpr (RS) {
@@ -340,11 +343,11 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
             n_out = (long long)kn + (long long)nz * (ie + (long long)nx * jn);
             m_out = mask ? mask[n_out] : (uint8_t)0;
             if (m_out) epi_copy(0, u, n_out);
-            if (need_b) epi_copy(1, epi.b, n_out);
-            if (mode == PF_EPI_JACOBI || need_xa) epi_copy(2, epi.x, n_out);
-            if (need_d) epi_copy(3, epi.dinv, n_out);
-            if (need_xa) epi_copy(4, epi.xadd, n_out);
-            if (need_dot) epi_copy(5, epi.dot_a, n_out);
+            if constexpr (need_b) epi_copy(1, epi.b, n_out);
+            if constexpr (mode == PF_EPI_JACOBI || need_xa) epi_copy(2, epi.x, n_out);
+            if constexpr (need_d) epi_copy(3, epi.dinv, n_out);
+            if constexpr (need_xa) epi_copy(4, epi.xadd, n_out);
+            if constexpr (need_dot) epi_copy(5, epi.dot_a, n_out);
         }
         cp_async_commit();
         const T e = e_next;
@@ -401,9 +404,17 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
                 XST(1, 1, 0, a1, b1)
                 XST(2, 0, 1, a2, b2)
                 (void)a0;
-                const T o00 = fma(KC(0), b0, fma(KC(1), a1, KC(2) * a2));
-                const T o01 = fma(KC(1), b0, fma(KC(3), a1, KC(4) * a2));
-                const T o02 = fma(KC(2), b0, fma(KC(4), a1, KC(5) * a2));
+                T o00, o01, o02;
+                if constexpr (CM == 2) {  // cube: [[a,b,b],[b,a,b],[b,b,a]] v = (a - b) v + b sum(v)
+                    const T bs = KC(1) * (b0 + a1 + a2);
+                    o00 = fma(amb, b0, bs);
+                    o01 = fma(amb, a1, bs);
+                    o02 = fma(amb, a2, bs);
+                } else {
+                    o00 = fma(KC(0), b0, fma(KC(1), a1, KC(2) * a2));
+                    o01 = fma(KC(1), b0, fma(KC(3), a1, KC(4) * a2));
+                    o02 = fma(KC(2), b0, fma(KC(4), a1, KC(5) * a2));
+                }
                 const T o11 = fma(KC(6), b1, KC(7) * b2);
                 const T o12 = fma(KC(7), b1, KC(8) * b2);
                 XINV(0, 0, o00, o01, o02, T(0), o11, o12)
@@ -415,8 +426,14 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
                 (void)a1;
                 const T o00 = fma(KC(9), b0, KC(10) * a2);
                 const T o02 = fma(KC(10), b0, KC(11) * a2);
-                const T o10 = fma(KC(12), a0, KC(13) * b1);
-                const T o11 = fma(KC(13), a0, KC(14) * b1);
+                T o10, o11;
+                if constexpr (CM == 2) {  // cube: [[d,d],[d,d]]
+                    o10 = KC(12) * (a0 + b1);
+                    o11 = o10;
+                } else {
+                    o10 = fma(KC(12), a0, KC(13) * b1);
+                    o11 = fma(KC(13), a0, KC(14) * b1);
+                }
                 const T o12 = KC(15) * b2;
                 XINV(1, 0, o00, T(0), o02, o10, o11, o12)
             }
@@ -427,9 +444,15 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
                 (void)a2;
                 const T o00 = fma(KC(16), b0, KC(17) * a1);
                 const T o01 = fma(KC(17), b0, KC(18) * a1);
-                const T o10 = fma(KC(19), a0, KC(20) * b2);
+                T o10, o12;
+                if constexpr (CM == 2) {  // cube: components 0, 2 coupled by [[d,d],[d,d]]
+                    o10 = KC(19) * (a0 + b2);
+                    o12 = o10;
+                } else {
+                    o10 = fma(KC(19), a0, KC(20) * b2);
+                    o12 = fma(KC(20), a0, KC(21) * b2);
+                }
                 const T o11 = KC(22) * b1;
-                const T o12 = fma(KC(20), a0, KC(21) * b2);
                 XINV(0, 1, o00, o01, T(0), o10, o11, o12)
             }
             {  // pair (1,1): class 6 on 0 alone and 1, 2; class 7 full
@@ -437,11 +460,21 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
                 XST(1, 0, 1, a1, b1)
                 XST(2, 1, 0, a2, b2)
                 const T o00 = KC(26) * b0;
-                const T o01 = fma(KC(23), a1, KC(24) * a2);
-                const T o02 = fma(KC(24), a1, KC(25) * a2);
-                const T o10 = fma(KC(27), a0, fma(KC(28), b1, KC(29) * b2));
-                const T o11 = fma(KC(28), a0, fma(KC(30), b1, KC(31) * b2));
-                const T o12 = fma(KC(29), a0, fma(KC(31), b1, KC(32) * b2));
+                T o01, o02, o10, o11, o12;
+                if constexpr (CM == 2) {  // cube: class 6 [[d,d],[d,d]] on 1, 2; class 7 circulant
+                    o01 = KC(23) * (a1 + a2);
+                    o02 = o01;
+                    const T gs = KC(28) * (a0 + b1 + b2);
+                    o10 = fma(fmg, a0, gs);
+                    o11 = fma(fmg, b1, gs);
+                    o12 = fma(fmg, b2, gs);
+                } else {
+                    o01 = fma(KC(23), a1, KC(24) * a2);
+                    o02 = fma(KC(24), a1, KC(25) * a2);
+                    o10 = fma(KC(27), a0, fma(KC(28), b1, KC(29) * b2));
+                    o11 = fma(KC(28), a0, fma(KC(30), b1, KC(31) * b2));
+                    o12 = fma(KC(29), a0, fma(KC(31), b1, KC(32) * b2));
+                }
                 XINV(1, 1, o00, o01, o02, o10, o11, o12)
             }
 #undef XINV
@@ -485,15 +518,15 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
                 T y = P1[c] + s_x[s & 1][c][w + 1][l];
                 if (m_out & (1 << c)) y = s_ep[0][c][tid];
                 T o = y;
-                if (mode == PF_EPI_RESID) {
+                if constexpr (mode == PF_EPI_RESID) {
                     o = s_ep[1][c][tid] - y;
-                } else if (mode == PF_EPI_JACOBI) {
+                } else if constexpr (mode == PF_EPI_JACOBI) {
                     o = s_ep[2][c][tid] + wgt * s_ep[3][c][tid] * (s_ep[1][c][tid] - y);
-                } else if (mode == PF_EPI_JACOBI_ADD) {
+                } else if constexpr (mode == PF_EPI_JACOBI_ADD) {
                     o = s_ep[4][c][tid] + s_ep[2][c][tid] + wgt * s_ep[3][c][tid] * (s_ep[1][c][tid] - y);
                 }
                 epi.out[3 * n_out + c] = o;
-                if (need_dot) dot += (double)s_ep[5][c][tid] * (double)(epi.dot_of_y ? y : o);
+                if constexpr (need_dot) dot += (double)s_ep[5][c][tid] * (double)(epi.dot_of_y ? y : o);
             }
         }
 #pragma unroll
@@ -504,7 +537,7 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
                 for (int b = 0; b < 2; b++) glo[c][a][b] = ghi[c][a][b];
     }
 #undef BK
-    if (epi.dot_partial) {
+    if constexpr (DOT) {
         const double sblk = block_sum<NT>(dot, s_red);
         if (threadIdx.x == 0)
             epi.dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = sblk;
@@ -612,6 +645,35 @@ long long q4_num_blocks(const Grid& g) { return (g.n_nodes + 255) / 256; }
 // ---------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------
+template <typename T, typename TE, int TY, int CM, int MODE, bool DOT>
+static int h8_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
+                     const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, cudaStream_t st) {
+    PF_CUDA(launch_pdl(k_matvec_h8<T, TE, TY, CM, MODE, DOT>, dim3(grid), dim3((TY + 1) * 32), 0, st, g.nel[0], g.nel[1],
+                       g.nel[2], cx, u, E, mask, blk, cf, epi));
+    return PF_OK;
+}
+
+template <typename T, typename TE, int TY, int CM>
+static int h8_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
+                       const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, bool dot, cudaStream_t st) {
+#define PF_H8(M, D) return h8_launch<T, TE, TY, CM, M, D>(grid, cx, g, u, E, mask, blk, cf, epi, st)
+    switch (epi.mode) {
+        case PF_EPI_STORE:
+            if (dot) PF_H8(PF_EPI_STORE, true);
+            PF_H8(PF_EPI_STORE, false);
+        case PF_EPI_RESID:
+            if (dot) PF_H8(PF_EPI_RESID, true);
+            PF_H8(PF_EPI_RESID, false);
+        case PF_EPI_JACOBI:
+            if (dot) PF_H8(PF_EPI_JACOBI, true);
+            PF_H8(PF_EPI_JACOBI, false);
+        default:
+            if (dot) PF_H8(PF_EPI_JACOBI_ADD, true);
+            PF_H8(PF_EPI_JACOBI_ADD, false);
+    }
+#undef PF_H8
+}
+
 template <typename T, typename TE>
 int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mask, const Epi<T>& epi,
                        cudaStream_t st) {
@@ -634,12 +696,14 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
         const H8Blk<T> blk = make_blk<T>(op);
         pf::count_launch();
         constexpr int CMS = sizeof(T) == 4 ? 1 : 2;  // the sparse variant of this precision
+        const bool dot = epi.dot_partial != nullptr;
+        if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");
+        int s;
         if (cm != 0)
-            PF_CUDA(launch_pdl(k_matvec_h8<T, TE, TY, CMS>, dim3(grid), dim3((TY + 1) * 32), 0, st, g.nel[0], g.nel[1], g.nel[2], cx, u, E,
-                                                                      mask, blk, cf, epi));
+            s = h8_dispatch<T, TE, TY, CMS>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
         else
-            PF_CUDA(launch_pdl(k_matvec_h8<T, TE, TY, 0>, dim3(grid), dim3((TY + 1) * 32), 0, st, g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask,
-                                                                    blk, cf, epi));
+            s = h8_dispatch<T, TE, TY, 0>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+        if (s) return s;
     } else {
         const long long nb = q4_num_blocks(g);
         pf::count_launch();
