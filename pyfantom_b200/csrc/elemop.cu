@@ -544,6 +544,342 @@ __global__ void __launch_bounds__((TY + 1) * 32, 3)
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// 3D matvec: register x-march
+// ---------------------------------------------------------------------------------------
+// One element per thread and step.  Warp w of a block computes element row
+// je = jy0 - 1 + w, lane l element column ke = kz0 - 1 + l (lanes 0..30; lane 31 only
+// supplies its node column to lane 30).  Each lane reads its own node column of rows je
+// and je + 1 straight from global memory into registers one plane ahead (a warp reads 32
+// consecutive nodes of a row: coalesced), forms the y stage of the face transform of that
+// column and takes the z neighbour's by shuffle, so the forward path uses neither shared
+// memory nor a barrier.  On the way back the z neighbour's corner arrives by shuffle and the
+// contribution to node row je goes to the warp below through one shared-memory exchange,
+// the only barrier of the step.  Warps 0..NW-2 own node rows jy0 .. jy0+NW-2 and lanes
+// 0..29 node columns kz0 .. kz0+29.  For a cube element (CM 2) the element's scale is
+// folded into the seven coefficient values instead of the 24 transformed inputs.
+// Loaded values are never copied between registers before use (a copy would wait for the
+// load): the constraint bytes stay separate until the next step and each element scale is
+// loaded straight into its register once the current one is spent.  (Unrolling the march by
+// two to alternate register sets, or prefetching two planes ahead, measured slower: more
+// registers, fewer resident warps.)
+constexpr int kZTileR = 30;
+
+// Element operator in the Walsh basis.  glo / ghi: transformed lower / upper faces (yz
+// stages done); e: the element's scale.  Returns in G the lower-face outputs plus the
+// upper-face outputs of the previous element (carry), and leaves this element's upper-face
+// outputs in carry.  Classes are taken in (y, z) parity pairs: the pair p = (0,py,pz),
+// (1,py,pz) reads and writes exactly the modes (c=0: py,pz), (c=1: py^1,pz), (c=2: py,pz^1).
+template <typename T, int CM>
+__device__ __forceinline__ void h8_element(const T (&glo)[3][2][2], const T (&ghi)[3][2][2], T e,
+                                           const H8Coef<T>& cf, const volatile T* vb, T (&carry)[3][2][2],
+                                           T (&G)[3][2][2]) {
+    // x stage of slot (component c, y-mode ym, z-mode zm): A = x-mode 0, B = x-mode 1
+#define XST(c, ym, zm, A, B)                                                                  \
+    const T A = (CM == 2) ? ghi[c][ym][zm] + glo[c][ym][zm] : e * (ghi[c][ym][zm] + glo[c][ym][zm]); \
+    const T B = (CM == 2) ? ghi[c][ym][zm] - glo[c][ym][zm] : e * (ghi[c][ym][zm] - glo[c][ym][zm]);
+    // inverse x stage for pair (py, pz): class p0 outputs o0*, class p1 outputs o1*
+#define XINV(py, pz, o00, o01, o02, o10, o11, o12)                 \
+    G[0][py][pz] = ((o10) - (o00)) + carry[0][py][pz];             \
+    carry[0][py][pz] = (o10) + (o00);                              \
+    G[1][(py) ^ 1][pz] = ((o01) - (o11)) + carry[1][(py) ^ 1][pz]; \
+    carry[1][(py) ^ 1][pz] = (o01) + (o11);                        \
+    G[2][py][(pz) ^ 1] = ((o02) - (o12)) + carry[2][py][(pz) ^ 1]; \
+    carry[2][py][(pz) ^ 1] = (o02) + (o12);
+    if constexpr (CM == 2) {
+        // cube element: values a-b, b, c, d, e, f-g, g, each times the element scale
+        const T kA = e * cf.c[0], kB = e * cf.c[1], kC = e * cf.c[2], kD = e * cf.c[3];
+        const T kE = e * cf.c[4], kF = e * cf.c[5], kG = e * cf.c[6];
+        {  // pair (0,0): class 0 circulant on (b0, a1, a2); class 1 [[b,c],[c,b]] on (b1, b2)
+            XST(0, 0, 0, a0, b0)
+            XST(1, 1, 0, a1, b1)
+            XST(2, 0, 1, a2, b2)
+            (void)a0;
+            const T bs = kB * (b0 + a1 + a2);
+            const T o00 = fma(kA, b0, bs), o01 = fma(kA, a1, bs), o02 = fma(kA, a2, bs);
+            const T o11 = fma(kB, b1, kC * b2), o12 = fma(kC, b1, kB * b2);
+            XINV(0, 0, o00, o01, o02, T(0), o11, o12)
+        }
+        {  // pair (1,0): class 2 [[b,c],[c,b]] on (b0, a2); class 3 d on (a0, b1), e on b2
+            XST(0, 1, 0, a0, b0)
+            XST(1, 0, 0, a1, b1)
+            XST(2, 1, 1, a2, b2)
+            (void)a1;
+            const T o00 = fma(kB, b0, kC * a2), o02 = fma(kC, b0, kB * a2);
+            const T o10 = kD * (a0 + b1);
+            const T o12 = kE * b2;
+            XINV(1, 0, o00, T(0), o02, o10, o10, o12)
+        }
+        {  // pair (0,1): class 4 [[b,c],[c,b]] on (b0, a1); class 5 d on (a0, b2), e on b1
+            XST(0, 0, 1, a0, b0)
+            XST(1, 1, 1, a1, b1)
+            XST(2, 0, 0, a2, b2)
+            (void)a2;
+            const T o00 = fma(kB, b0, kC * a1), o01 = fma(kC, b0, kB * a1);
+            const T o10 = kD * (a0 + b2);
+            const T o11 = kE * b1;
+            XINV(0, 1, o00, o01, T(0), o10, o11, o10)
+        }
+        {  // pair (1,1): class 6 e on b0, d on (a1, a2); class 7 circulant on (a0, b1, b2)
+            XST(0, 1, 1, a0, b0)
+            XST(1, 0, 1, a1, b1)
+            XST(2, 1, 0, a2, b2)
+            const T o00 = kE * b0;
+            const T o01 = kD * (a1 + a2);
+            const T gs = kG * (a0 + b1 + b2);
+            const T o10 = fma(kF, a0, gs), o11 = fma(kF, b1, gs), o12 = fma(kF, b2, gs);
+            XINV(1, 1, o00, o01, o01, o10, o11, o12)
+        }
+    } else if constexpr (CM == 1) {
+#define KC(q) cf.c[q]
+        {
+            XST(0, 0, 0, a0, b0)
+            XST(1, 1, 0, a1, b1)
+            XST(2, 0, 1, a2, b2)
+            (void)a0;
+            const T o00 = fma(KC(0), b0, fma(KC(1), a1, KC(2) * a2));
+            const T o01 = fma(KC(1), b0, fma(KC(3), a1, KC(4) * a2));
+            const T o02 = fma(KC(2), b0, fma(KC(4), a1, KC(5) * a2));
+            const T o11 = fma(KC(6), b1, KC(7) * b2);
+            const T o12 = fma(KC(7), b1, KC(8) * b2);
+            XINV(0, 0, o00, o01, o02, T(0), o11, o12)
+        }
+        {
+            XST(0, 1, 0, a0, b0)
+            XST(1, 0, 0, a1, b1)
+            XST(2, 1, 1, a2, b2)
+            (void)a1;
+            const T o00 = fma(KC(9), b0, KC(10) * a2);
+            const T o02 = fma(KC(10), b0, KC(11) * a2);
+            const T o10 = fma(KC(12), a0, KC(13) * b1);
+            const T o11 = fma(KC(13), a0, KC(14) * b1);
+            const T o12 = KC(15) * b2;
+            XINV(1, 0, o00, T(0), o02, o10, o11, o12)
+        }
+        {
+            XST(0, 0, 1, a0, b0)
+            XST(1, 1, 1, a1, b1)
+            XST(2, 0, 0, a2, b2)
+            (void)a2;
+            const T o00 = fma(KC(16), b0, KC(17) * a1);
+            const T o01 = fma(KC(17), b0, KC(18) * a1);
+            const T o10 = fma(KC(19), a0, KC(20) * b2);
+            const T o12 = fma(KC(20), a0, KC(21) * b2);
+            const T o11 = KC(22) * b1;
+            XINV(0, 1, o00, o01, T(0), o10, o11, o12)
+        }
+        {
+            XST(0, 1, 1, a0, b0)
+            XST(1, 0, 1, a1, b1)
+            XST(2, 1, 0, a2, b2)
+            const T o00 = KC(26) * b0;
+            const T o01 = fma(KC(23), a1, KC(24) * a2);
+            const T o02 = fma(KC(24), a1, KC(25) * a2);
+            const T o10 = fma(KC(27), a0, fma(KC(28), b1, KC(29) * b2));
+            const T o11 = fma(KC(28), a0, fma(KC(30), b1, KC(31) * b2));
+            const T o12 = fma(KC(29), a0, fma(KC(31), b1, KC(32) * b2));
+            XINV(1, 1, o00, o01, o02, o10, o11, o12)
+        }
+#undef KC
+    } else {
+        // any reflection-symmetric K0: dense 3x3 class blocks re-read from shared memory
+#define BK(p, i, j) vb[(p) * 9 + (i) * 3 + (j)]
+#pragma unroll
+        for (int pyz = 0; pyz < 4; pyz++) {
+            const int py = pyz & 1, pz = pyz >> 1;
+            const int p0 = 2 * py + 4 * pz, p1 = p0 + 1;
+            const T h0 = e * ghi[0][py][pz], h1 = e * ghi[1][py ^ 1][pz], h2 = e * ghi[2][py][pz ^ 1];
+            const T a0 = fma(e, glo[0][py][pz], h0), b0 = fma(-e, glo[0][py][pz], h0);
+            const T a1 = fma(e, glo[1][py ^ 1][pz], h1), b1 = fma(-e, glo[1][py ^ 1][pz], h1);
+            const T a2 = fma(e, glo[2][py][pz ^ 1], h2), b2 = fma(-e, glo[2][py][pz ^ 1], h2);
+            const T o00 = fma(BK(p0, 0, 0), b0, fma(BK(p0, 0, 1), a1, BK(p0, 0, 2) * a2));
+            const T o01 = fma(BK(p0, 1, 0), b0, fma(BK(p0, 1, 1), a1, BK(p0, 1, 2) * a2));
+            const T o02 = fma(BK(p0, 2, 0), b0, fma(BK(p0, 2, 1), a1, BK(p0, 2, 2) * a2));
+            const T o10 = fma(BK(p1, 0, 0), a0, fma(BK(p1, 0, 1), b1, BK(p1, 0, 2) * b2));
+            const T o11 = fma(BK(p1, 1, 0), a0, fma(BK(p1, 1, 1), b1, BK(p1, 1, 2) * b2));
+            const T o12 = fma(BK(p1, 2, 0), a0, fma(BK(p1, 2, 1), b1, BK(p1, 2, 2) * b2));
+            G[0][py][pz] = (o10 - o00) + carry[0][py][pz];
+            carry[0][py][pz] = o10 + o00;
+            G[1][py ^ 1][pz] = (o01 - o11) + carry[1][py ^ 1][pz];
+            carry[1][py ^ 1][pz] = o01 + o11;
+            G[2][py][pz ^ 1] = (o02 - o12) + carry[2][py][pz ^ 1];
+            carry[2][py][pz ^ 1] = o02 + o12;
+        }
+#undef BK
+    }
+#undef XINV
+#undef XST
+}
+
+template <typename T, typename TE, int NW, int MINB, int CM, int MODE, bool DOT>
+__global__ void __launch_bounds__(NW * 32, MINB)
+    k_matvec_h8r(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
+                 const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
+    pdl_wait();
+    pdl_trigger();
+    constexpr int TY = NW - 1, NT = NW * 32;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ T s_q[2][3][NW][32];
+    __shared__ double s_red[NW];
+    __shared__ T s_blk[72];
+    if (epi.skip && *epi.skip) return;
+    constexpr int mode = MODE;
+    constexpr bool need_b = mode != PF_EPI_STORE, need_x = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
+    constexpr bool need_xa = mode == PF_EPI_JACOBI_ADD;
+    const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int kz0 = blockIdx.x * kZTileR, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
+    const int je = jy0 - 1 + w, kc = kz0 - 1 + l;  // element row; node column of its lower z corner
+    const bool col_ok = kc >= 0 && kc < nz;
+    const bool ok0 = col_ok && je >= 0 && je < ny, ok1 = col_ok && je + 1 < ny;
+    const bool elem_ok = l < 31 && je >= 0 && je < NY && kc >= 0 && kc < NZ;
+    const bool owner = w < TY && l < kZTileR && je + 1 < ny && kc + 1 < nz;
+    // 32-bit node and element indices (the launcher checks 3 * nodes < 2^31)
+    const int rows = nz * nx;        // nodes per node row (y)
+    const int n0 = kc + rows * je;   // node (je, 0, kc): rows je, je + 1 advance by nz per plane
+    const int n1 = n0 + rows;
+    const int eplane = NY * NZ;      // elements per element plane (x)
+    const int e0 = je * NZ + kc;     // element (0, je, kc)
+    const bool has_mask = mask != nullptr;
+    const T wgt = epi_omega(epi);
+    double dot = 0.0;
+    if (CM == 0 && tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
+    const volatile T* vb = s_blk;
+
+    // node values of this lane's column in rows je, je+1 of plane p (zero outside the mesh)
+    // and the two constraint bytes; nothing here waits for the loads
+    auto load = [&](int p, T (&v)[2][3], int& m0, int& m1) {
+        const bool pok = p >= 0 && p < nx;
+        const int a0 = n0 + nz * p, a1 = n1 + nz * p;
+        m0 = 0;
+        m1 = 0;
+        if (pok && ok0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[0][c] = u[3 * a0 + c];
+            if (has_mask) m0 = mask[a0];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[0][c] = T(0);
+        }
+        if (pok && ok1) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[1][c] = u[3 * a1 + c];
+            if (has_mask) m1 = mask[a1];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[1][c] = T(0);
+        }
+    };
+    // y stage of this column, z stage with the next column's (shuffle): transformed face
+    auto face = [&](T (&v)[2][3], int m0, int m1, T (&g)[3][2][2]) {
+        if (__any_sync(FULL, m0 | m1)) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if ((m0 >> c) & 1) v[0][c] = T(0);
+                if ((m1 >> c) & 1) v[1][c] = T(0);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const T s = v[1][c] + v[0][c], d = v[1][c] - v[0][c];
+            const T sn = __shfl_down_sync(FULL, s, 1), dn = __shfl_down_sync(FULL, d, 1);
+            g[c][0][0] = s + sn;
+            g[c][0][1] = sn - s;
+            g[c][1][0] = d + dn;
+            g[c][1][1] = dn - d;
+        }
+    };
+    auto escale = [&](int ie) -> T { return (elem_ok && ie >= 0 && ie < NX) ? (T)E[e0 + eplane * ie] : T(0); };
+
+    // One step (element ie = ix0 - 1 + s).
+    //   v, m0, m1: plane ie+1 (loaded one step earlier); refilled with plane ie+2
+    //   e: scale of element ie; refilled with that of element ie+1 after its last use
+    T carry[3][2][2];
+    auto step = [&](int s, T (&gl)[3][2][2], T (&gh)[3][2][2], T (&v)[2][3], int& m0, int& m1, T& e) {
+        const int ie = ix0 - 1 + s;
+        face(v, m0, m1, gh);
+        if (s < CXc) load(ie + 2, v, m0, m1);
+        // epilogue operands of the owned node (je+1, ie, kc+1): consumed after the barrier
+        const bool out_now = owner && s >= 1 && ie < nx;
+        const int no = n1 + 1 + nz * ie;
+        T pb[3], px[3], pd[3], pa[3], pt[3];
+        int mo = 0;
+        if (out_now) {
+            if (has_mask) mo = mask[no];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if constexpr (need_b) pb[c] = epi.b[3 * no + c];
+                if constexpr (need_x) px[c] = epi.x[3 * no + c];
+                if constexpr (need_x) pd[c] = epi.dinv[3 * no + c];
+                if constexpr (need_xa) pa[c] = epi.xadd[3 * no + c];
+                if constexpr (DOT) pt[c] = epi.dot_a[3 * no + c];
+            }
+        }
+        T G[3][2][2];
+        h8_element<T, CM>(gl, gh, e, cf, vb, carry, G);
+        e = (s < CXc) ? escale(ie + 1) : T(0);
+        // inverse y and z stages; node (je+1, kc+1) from this lane and the next, the row je
+        // part to the warp below
+        T P1[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const T r0a = G[c][0][0] - G[c][1][0], r0b = G[c][0][1] - G[c][1][1];
+            const T r1a = G[c][0][0] + G[c][1][0], r1b = G[c][0][1] + G[c][1][1];
+            const T lo0 = r0a - r0b, up0 = r0a + r0b, lo1 = r1a - r1b, up1 = r1a + r1b;
+            P1[c] = up1 + __shfl_down_sync(FULL, lo1, 1);
+            s_q[s & 1][c][w][l] = up0 + __shfl_down_sync(FULL, lo0, 1);
+        }
+        __syncthreads();
+        if (out_now) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                T y = P1[c] + s_q[s & 1][c][w + 1][l];
+                if ((mo >> c) & 1) y = u[3 * no + c];
+                T o = y;
+                if constexpr (mode == PF_EPI_RESID) {
+                    o = pb[c] - y;
+                } else if constexpr (mode == PF_EPI_JACOBI) {
+                    o = px[c] + wgt * pd[c] * (pb[c] - y);
+                } else if constexpr (mode == PF_EPI_JACOBI_ADD) {
+                    o = pa[c] + px[c] + wgt * pd[c] * (pb[c] - y);
+                }
+                epi.out[3 * no + c] = o;
+                if constexpr (DOT) dot += (double)pt[c] * (double)(epi.dot_of_y ? y : o);
+            }
+        }
+    };
+
+    T gA[3][2][2], gB[3][2][2];
+    T vA[2][3];
+    int mA0, mA1;
+    load(ix0 - 1, vA, mA0, mA1);
+    face(vA, mA0, mA1, gA);
+    load(ix0, vA, mA0, mA1);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) carry[c][a][b] = T(0);
+    T eA = escale(ix0 - 1);
+    if (CM == 0) __syncthreads();
+    for (int s = 0; s <= CXc; s++) {
+        step(s, gA, gB, vA, mA0, mA1, eA);
+        // the upper face becomes the next lower face (computed values: no wait)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int b = 0; b < 2; b++) gA[c][a][b] = gB[c][a][b];
+    }
+    if constexpr (DOT) {
+        const double sblk = block_sum<NT>(dot, s_red);
+        if (threadIdx.x == 0)
+            epi.dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = sblk;
+    }
+}
+
 template <typename T>
 static H8Blk<T> make_blk(const Op* op) {
     H8Blk<T> b;
@@ -569,10 +905,43 @@ static void h8_launch_dims(const Grid& g, int TY, bool fp32, dim3* grid, int* CX
     *grid = dim3(tz, ty, (nx + cx - 1) / cx);
 }
 
+// register x-march: NW warps per block (NW - 1 owned node rows), at least MINB blocks per SM
+// (FP64: 8 warps x 2 blocks, up to 128 registers; FP32: 12 warps x 2 blocks, up to 80;
+// FP32 with 9 warps x 3 blocks at 72 registers measured slower)
+constexpr int kNWr64 = 8, kMinBr64 = 2, kNWr32 = 12, kMinBr32 = 2;
+
+// the register x-march indexes nodes in 32 bits
+static bool h8r_fits(const Grid& g) { return 3LL * g.n_nodes < (1LL << 31) && g.n_elem < (1LL << 31); }
+
+// x-chunk length: fewest estimated block-steps, counting whole waves of the resident slots
+// (ties go to the longer chunk, which recomputes fewer boundary elements)
+static void h8r_launch_dims(const Grid& g, bool fp32, dim3* grid, int* CXc) {
+    const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
+    const int nw = fp32 ? kNWr32 : kNWr64;
+    const int tz = (nz + kZTileR - 1) / kZTileR, ty = (ny + nw - 2) / (nw - 1);
+    const long long slots = (long long)kNumSM * (fp32 ? kMinBr32 : kMinBr64);
+    const long long cols = (long long)tz * ty;
+    int best = 4;
+    long long best_cost = -1;
+    for (int cx = 4; cx <= 64; cx++) {
+        const long long nb = cols * ((nx + cx - 1) / cx);
+        const long long cost = ((nb + slots - 1) / slots) * (cx + 1);
+        if (best_cost < 0 || cost <= best_cost) {
+            best_cost = cost;
+            best = cx;
+        }
+    }
+    *CXc = best;
+    *grid = dim3(tz, ty, (nx + best - 1) / best);
+}
+
 long long h8_num_blocks(const Grid& g, int fp32) {
     dim3 gr;
     int cx;
-    h8_launch_dims(g, fp32 ? kTY32 : kTY64, fp32 != 0, &gr, &cx);
+    if (h8r_fits(g))
+        h8r_launch_dims(g, fp32 != 0, &gr, &cx);
+    else
+        h8_launch_dims(g, fp32 ? kTY32 : kTY64, fp32 != 0, &gr, &cx);
     return (long long)gr.x * gr.y * gr.z;
 }
 
@@ -653,6 +1022,36 @@ static int h8_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, 
     return PF_OK;
 }
 
+template <typename T, typename TE, int CM, int MODE, bool DOT>
+static int h8r_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
+                      const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, cudaStream_t st) {
+    constexpr int MINB = sizeof(T) == 8 ? kMinBr64 : kMinBr32, NW = sizeof(T) == 8 ? kNWr64 : kNWr32;
+    PF_CUDA(launch_pdl(k_matvec_h8r<T, TE, NW, MINB, CM, MODE, DOT>, dim3(grid), dim3(NW * 32), 0, st,
+                       g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask, blk, cf, epi));
+    return PF_OK;
+}
+
+template <typename T, typename TE, int CM>
+static int h8r_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
+                        const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, bool dot, cudaStream_t st) {
+#define PF_H8R(M, D) return h8r_launch<T, TE, CM, M, D>(grid, cx, g, u, E, mask, blk, cf, epi, st)
+    switch (epi.mode) {
+        case PF_EPI_STORE:
+            if (dot) PF_H8R(PF_EPI_STORE, true);
+            PF_H8R(PF_EPI_STORE, false);
+        case PF_EPI_RESID:
+            if (dot) PF_H8R(PF_EPI_RESID, true);
+            PF_H8R(PF_EPI_RESID, false);
+        case PF_EPI_JACOBI:
+            if (dot) PF_H8R(PF_EPI_JACOBI, true);
+            PF_H8R(PF_EPI_JACOBI, false);
+        default:
+            if (dot) PF_H8R(PF_EPI_JACOBI_ADD, true);
+            PF_H8R(PF_EPI_JACOBI_ADD, false);
+    }
+#undef PF_H8R
+}
+
 template <typename T, typename TE, int TY, int CM>
 static int h8_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
                        const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, bool dot, cudaStream_t st) {
@@ -695,6 +1094,33 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
             for (int v = 0; v < 7; v++) cf.c[v] = (T)op->cube_v[v];
         const H8Blk<T> blk = make_blk<T>(op);
         pf::count_launch();
+        if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");
+        if (h8r_fits(g)) {
+            // register x-march: a cube element's seven values (a-b, b, c, d, e, f-g, g), the
+            // 33 nonzeros of another isotropic box, or the dense blocks
+            const int cmr = op->cube ? 2 : (op->sparse ? 1 : 0);
+            H8Coef<T> cr;
+            for (int q = 0; q < 33; q++) cr.c[q] = T(0);
+            if (cmr == 2) {
+                const double* v = op->cube_v;
+                const double vals[7] = {v[0] - v[1], v[1], v[2], v[3], v[4], v[5] - v[6], v[6]};
+                for (int q = 0; q < 7; q++) cr.c[q] = (T)vals[q];
+            } else if (cmr == 1) {
+                for (int q = 0; q < 33; q++) cr.c[q] = (T)op->coef[q];
+            }
+            h8r_launch_dims(g, sizeof(T) == 4, &grid, &cx);
+            const bool dot = epi.dot_partial != nullptr;
+            int s;
+            if (cmr == 2)
+                s = h8r_dispatch<T, TE, 2>(grid, cx, g, u, E, mask, blk, cr, epi, dot, st);
+            else if (cmr == 1)
+                s = h8r_dispatch<T, TE, 1>(grid, cx, g, u, E, mask, blk, cr, epi, dot, st);
+            else
+                s = h8r_dispatch<T, TE, 0>(grid, cx, g, u, E, mask, blk, cr, epi, dot, st);
+            if (s) return s;
+            PF_LAUNCH_CHECK("fine matvec launch");
+            return PF_OK;
+        }
         constexpr int CMS = sizeof(T) == 4 ? 1 : 2;  // the sparse variant of this precision
         const bool dot = epi.dot_partial != nullptr;
         if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");

@@ -506,7 +506,9 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     s = s ? s : dalloc((void**)&mg->r, n0 * sizeof(double));
     s = s ? s : dalloc((void**)&mg->p, n0 * sizeof(double));
     s = s ? s : dalloc((void**)&mg->q, n0 * sizeof(double));
-    long long np = fine_matvec_num_blocks(op, mg->fp32);
+    // partial sums of the FP64 PCG matvec and (mixed form) of the FP32 V-cycle matvec
+    long long np = fine_matvec_num_blocks(op, 0);
+    if (mg->fp32 && fine_matvec_num_blocks(op, 1) > np) np = fine_matvec_num_blocks(op, 1);
     if (np < 8 * kNumSM) np = 8 * kNumSM;
     for (int l = 1; l < mg->nlev; l++) np = np > stencil_matvec_num_blocks(mg->L[l].g) ? np : stencil_matvec_num_blocks(mg->L[l].g);
     mg->npartials = np;
