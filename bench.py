@@ -224,7 +224,7 @@ def run_ours(args, rank, world, local_rank):
     hbm, peak_kind = peaks()
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
-            "kernel": "k_matvec_h8<double> (fine-level stiffness matvec with fused epilogues)",
+            "kernel": "k_matvec_h8r<double> (fine-level stiffness matvec, register x-march, fused epilogues)",
             "launches_in_solve": int(n_l.value), "avg_launch_us": round(avg_us, 2),
             "algorithmic_bytes_per_launch": round(byts.value / max(n_l.value, 1))}
     prof_path = os.path.join(ROOT, "profiles", "matvec_h8_traffic.json")

@@ -799,24 +799,31 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         const int ie = ix0 - 1 + s;
         face(v, m0, m1, gh);
         if (s < CXc) load(ie + 2, v, m0, m1);
-        // epilogue operands of the owned node (je+1, ie, kc+1): consumed after the barrier
+        // epilogue operands of the owned node (je+1, ie, kc+1), consumed after the barrier:
+        // loaded before the element operator, except the three Jacobi vectors in FP64, which
+        // are loaded after it (held across it they would spill)
         const bool out_now = owner && s >= 1 && ie < nx;
         const int no = n1 + 1 + nz * ie;
         T pb[3], px[3], pd[3], pa[3], pt[3];
         int mo = 0;
-        if (out_now) {
-            if (has_mask) mo = mask[no];
+        constexpr bool late = sizeof(T) == 8 && need_x;
+        auto fetch = [&]() {
+            if (out_now) {
+                if (has_mask) mo = mask[no];
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                if constexpr (need_b) pb[c] = epi.b[3 * no + c];
-                if constexpr (need_x) px[c] = epi.x[3 * no + c];
-                if constexpr (need_x) pd[c] = epi.dinv[3 * no + c];
-                if constexpr (need_xa) pa[c] = epi.xadd[3 * no + c];
-                if constexpr (DOT) pt[c] = epi.dot_a[3 * no + c];
+                for (int c = 0; c < 3; c++) {
+                    if constexpr (need_b) pb[c] = epi.b[3 * no + c];
+                    if constexpr (need_x) px[c] = epi.x[3 * no + c];
+                    if constexpr (need_x) pd[c] = epi.dinv[3 * no + c];
+                    if constexpr (need_xa) pa[c] = epi.xadd[3 * no + c];
+                    if constexpr (DOT) pt[c] = epi.dot_a[3 * no + c];
+                }
             }
-        }
+        };
+        if constexpr (!late) fetch();
         T G[3][2][2];
         h8_element<T, CM>(gl, gh, e, cf, vb, carry, G);
+        if constexpr (late) fetch();
         e = (s < CXc) ? escale(ie + 1) : T(0);
         // inverse y and z stages; node (je+1, kc+1) from this lane and the next, the row je
         // part to the warp below

@@ -199,7 +199,10 @@ template int launch_prolong<float>(const Grid&, const float*, float*, const int*
 // block q = o - c); a lower offset o < c uses the symmetry of the level operator,
 // A[n, o] = A[n+o, -o]^T, i.e. block q = c - o of the neighbour n+o, transposed.  The
 // neighbour's coefficients are read again by another block shortly after (from L2), so
-// DRAM carries each coefficient once: (NB+1)/2 blocks per node instead of NB.
+// DRAM carries each coefficient once: (NB+1)/2 blocks per node instead of NB.  The half
+// copy is tiled by 32 nodes, A[((n >> 5) * NH*BS + q*BS + a*DIM + b) * 32 + (n & 31)]:
+// each tile's (NB+1)/2 * DIM^2 coefficient rows are one contiguous run (16 KB in 3D FP32),
+// so DRAM streams through it instead of jumping between NH*BS planes of N values.
 // ---------------------------------------------------------------------------------------
 template <int DIM, typename T, bool HALF>
 __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
@@ -207,6 +210,7 @@ __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<
     pdl_wait();
     pdl_trigger();
     constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM, NG = NB / 3, C = NB / 2;
+    constexpr long long TS = (long long)(C + 1) * BS * 32;  // values per tile of the half copy
     __shared__ T s_part[NG][DIM][32];
     if (epi.skip && *epi.skip) return;
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -235,17 +239,17 @@ __global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<
                     for (int b = 0; b < DIM; b++)
                         acc[a] = fma(A[((long long)(o * BS + a * DIM + b)) * N + n], um[b], acc[a]);
             } else if (o >= C) {
-                const T* Aq = A + (long long)(o - C) * BS * N + n;
+                const T* Aq = A + (n >> 5) * TS + (o - C) * BS * 32 + (n & 31);
 #pragma unroll
                 for (int a = 0; a < DIM; a++)
 #pragma unroll
-                    for (int b = 0; b < DIM; b++) acc[a] = fma(Aq[(long long)(a * DIM + b) * N], um[b], acc[a]);
+                    for (int b = 0; b < DIM; b++) acc[a] = fma(Aq[(a * DIM + b) * 32], um[b], acc[a]);
             } else {
-                const T* Aq = A + (long long)(C - o) * BS * N + m;
+                const T* Aq = A + (m >> 5) * TS + (C - o) * BS * 32 + (m & 31);
 #pragma unroll
                 for (int a = 0; a < DIM; a++)
 #pragma unroll
-                    for (int b = 0; b < DIM; b++) acc[a] = fma(Aq[(long long)(b * DIM + a) * N], um[b], acc[a]);
+                    for (int b = 0; b < DIM; b++) acc[a] = fma(Aq[(b * DIM + a) * 32], um[b], acc[a]);
             }
         }
     }
@@ -301,13 +305,19 @@ template int launch_stencil_matvec<float>(const Grid&, const float*, const float
 // converted to the V-cycle precision
 template <typename T>
 __global__ void k_stencil_half(long long N, int nh, int bs, int c, const double* __restrict__ A, T* __restrict__ H) {
-    const long long total = N * nh * bs;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
-        H[i] = (T)A[i + (long long)c * bs * N];
+    // tiles of 32 nodes (the last one zero-padded): H[(t * nh*bs + qab) * 32 + lane]
+    const long long per_tile = (long long)nh * bs * 32;
+    const long long total = ((N + 31) / 32) * per_tile;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long t = i / per_tile;
+        const int r = (int)(i - t * per_tile), qab = r >> 5;
+        const long long n = t * 32 + (r & 31);
+        H[i] = n < N ? (T)A[(long long)(c * bs + qab) * N + n] : T(0);
+    }
 }
 long long stencil_half_size(const Grid& g) {
     const int nb = g.dim == 3 ? 27 : 9;
-    return g.n_nodes * ((nb + 1) / 2) * g.dof * g.dof;
+    return ((g.n_nodes + 31) / 32) * 32 * ((nb + 1) / 2) * g.dof * g.dof;
 }
 template <typename T>
 int launch_stencil_half(const Grid& g, const double* A, T* H, cudaStream_t st) {

@@ -18,7 +18,8 @@ int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaS
                     Jacobi0<TO> j0 = Jacobi0<TO>());
 template <typename T>
 int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStream_t st);
-// half = true: A is the half storage of launch_stencil_half (centre and upper offsets)
+// half = true: A is the half storage of launch_stencil_half (centre and upper offsets, in
+// tiles of 32 nodes)
 template <typename T>
 int launch_stencil_matvec(const Grid& g, const T* A, const T* u, const Epi<T>& epi, cudaStream_t st,
                           bool half = false);
