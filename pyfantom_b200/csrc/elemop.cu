@@ -6,13 +6,14 @@
 // (v = T u with T[(m,c),(l,c')] = delta_cc' prod_axis (m_axis ? +-1 : 1)) K0 becomes
 // block diagonal: B = T K0 T^T / 64 has eight 3x3 blocks, one per parity class
 // p = (px,py,pz), coupling component c in mode p ^ e_c.  K0 u = T^T B T u costs
-// 3 butterfly stages forward, 8 3x3 blocks and 3 stages back (~190 flops, against 576
-// multiply-adds for the dense 24x24 product).  The matvec kernel marches along x: warps
-// cover element rows in y, lanes cover element columns in z (the contiguous node axis),
-// so every plane of nodal values is read once, coalesced, into shared memory; the forward
-// and inverse y/z stages are done once per face and shared by the two elements on either
-// side of it; node sums across the tile use warp shuffles and one shared-memory exchange.
-// Owner-computes: each node of the tile is written once, no atomics, fixed summation order.
+// 3 butterfly stages forward, 8 3x3 blocks and 3 stages back (~150 flops for a cube
+// element, against 576 multiply-adds for the dense 24x24 product).  The matvec kernel
+// marches along x: warps cover element rows in y, lanes cover element columns in z (the
+// contiguous node axis); each lane reads its node column of two rows straight into
+// registers, the y/z stages of a face are done once and shared by the two elements on
+// either side of it along x, z neighbours are exchanged by shuffles and rows through one
+// shared-memory exchange per step.  Owner-computes: each node is written once, no atomics,
+// fixed summation order.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -119,430 +120,16 @@ int op_factorise(Op* op) {
 }
 
 // ---------------------------------------------------------------------------------------
-// 3D matvec: x-marching tile kernel
+// 3D matvec operands
 // ---------------------------------------------------------------------------------------
-// nodes owned per warp along z: FP32 (register staging) 30 of 32 loaded node columns,
-// FP64 (cp.async staging of 33 columns) 31
-constexpr int kZTile32 = 30, kZTile64 = 31;
-
 template <typename T>
 struct H8Blk {
     T b[8][3][3];
 };
 template <typename T>
 struct H8Coef {
-    T c[33];  // sparse coefficients (CM 1) or the 7 cube values (CM 2)
+    T c[33];  // the 33 sparse coefficients (CM 1) or the 7 cube values (CM 2)
 };
-// coefficient q of the sparse class blocks (CM 1: 33 values, CM 2: 7 cube values)
-template <int Q, int CM, typename T>
-__device__ __forceinline__ T coef(const H8Coef<T>& cf) {
-    if constexpr (CM == 2)
-        return cf.c[cube_index(Q)];
-    else
-        return cf.c[Q];
-}
-
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    if (bytes == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Pipelined x-march.  Step s (element layer ie = ix0-1+s):
-//   1. cp.async this thread's epilogue operands for its node of plane ie into its slots;
-//   2. forward stages of the plane ie+1 face (buffer (s+1)&1), element operator, inverse
-//      stages, node sums inside the warp (shuffles), exchange row sums in s_x[s&1];
-//   3. publish plane ie+2 (in registers since the previous step) to buffer s&1 (last read
-//      in step s-1), start loading plane ie+3, wait for the epilogue copies,
-//      __syncthreads (the only barrier of the step);
-//   4. owners finish their node of plane ie and apply the epilogue.
-// CM selects the element operator: 0 dense class blocks read from shared memory (any K0
-// with the reflection symmetry), 1 the 33 nonzeros of an isotropic box element, 2 the 7
-// values of a cube element (1, 2: coefficients held in registers).
-template <typename T, typename TE, int TY, int CM, int MODE, bool DOT>
-__global__ void __launch_bounds__((TY + 1) * 32, 3)
-    k_matvec_h8(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
-                const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
-    pdl_wait();
-    pdl_trigger();
-    constexpr int NW = TY + 1;
-    constexpr int NT = NW * 32;
-    constexpr int PR = TY + 2, PC = 33, NPE = PR * PC;
-    constexpr int NQ = (NPE + NT - 1) / NT;   // plane entries per thread (cp.async staging)
-    constexpr bool RS = sizeof(T) == 4;       // register staging (FP32) or cp.async (FP64)
-    constexpr int ZT = RS ? kZTile32 : kZTile64;
-    constexpr int NSLOT = 6;                 // u (identity rows), b, x, dinv, xadd, dot_a
-    __shared__ __align__(16) T s_u[2][3][PR][PC];
-    __shared__ T s_x[2][3][NW][32];
-    __shared__ __align__(16) T s_ep[NSLOT][3][NT];
-    __shared__ double s_red[NW];
-    __shared__ T s_blk[8 * 9];
-    if (epi.skip && *epi.skip) return;
-    const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
-    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int kz0 = blockIdx.x * ZT, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
-    const int je = jy0 - 1 + w, ke = kz0 - 1 + l;
-    const int jn = jy0 + w, kn = kz0 + l;
-    const bool owner = (w < TY) && (l < ZT) && (jn < ny) && (kn < nz);
-    const bool col_ok = (l <= ZT) && (je >= 0) && (je < NY) && (ke >= 0) && (ke < NZ);
-    const T wgt = epi_omega(epi);
-    // the epilogue mode and the fused dot are compile-time: no per-step branches on them
-    constexpr int mode = MODE;
-    constexpr bool need_b = mode != PF_EPI_STORE, need_d = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
-    constexpr bool need_xa = mode == PF_EPI_JACOBI_ADD, need_dot = DOT;
-    double dot = 0.0;
-    constexpr int TB_ = (int)sizeof(T);
-
-    // FP64: cp.async copies of whole plane tiles (33 node columns, 31 owned per warp).
-    // issue the copies of plane p into buffer buf; returns the masks of the entries issued
-    [[maybe_unused]] auto issue_plane = [&](int p, int buf, uint8_t* mq) {
-#pragma unroll
-        for (int q = 0; q < NQ; q++) {
-            const int idx = tid + q * NT;
-            mq[q] = 0;
-            if (idx < NPE) {
-                const int r = idx / PC, c = idx - r * PC;
-                const int j = jy0 - 1 + r, k = kz0 - 1 + c;
-                if (p >= 0 && p < nx && j >= 0 && j < ny && k >= 0 && k < nz) {
-                    const long long n = (long long)k + (long long)nz * (p + (long long)nx * j);
-                    mq[q] = mask ? mask[n] : (uint8_t)0;
-#pragma unroll
-                    for (int d = 0; d < 3; d++) cp_async(&s_u[buf][d][r][c], u + 3 * n + d, TB_);
-                } else {
-#pragma unroll
-                    for (int d = 0; d < 3; d++) s_u[buf][d][r][c] = T(0);
-                }
-            }
-        }
-    };
-    [[maybe_unused]] auto fix_plane = [&](int buf, const uint8_t* mq) {
-#pragma unroll
-        for (int q = 0; q < NQ; q++) {
-            const int idx = tid + q * NT;
-            if (idx < NPE && mq[q]) {
-                const int r = idx / PC, c = idx - r * PC;
-#pragma unroll
-                for (int d = 0; d < 3; d++)
-                    if (mq[q] & (1 << d)) s_u[buf][d][r][c] = T(0);
-            }
-        }
-    };
-    // FP32: plane staging through registers: thread (w, l) loads node (jy0 - 1 + w, kz0 - 1 + l) of a plane into
-    // registers one step ahead (coalesced: a warp reads 32 consecutive nodes), zeroes its
-    // constrained components (skipped columns) and publishes it to row w, column l of a
-    // plane buffer; the last warp also carries the row jy0 + TY above the tile.  Lanes
-    // 0..30 compute the elements kz0-1 .. kz0+29 and own the nodes kz0 .. kz0+29; lane 31
-    // is inactive and reads column 32, which is zero and never written.
-    const int jo = jy0 - 1 + w, ko = kz0 - 1 + l, jx = jy0 + TY;
-    const bool own_ok = jo >= 0 && jo < ny && ko >= 0 && ko < nz;
-    const bool ext_ok = jx < ny && ko >= 0 && ko < nz;
-    T rv[3], rx[3];
-    uint8_t rm = 0, rxm = 0;
-    [[maybe_unused]] auto load_plane = [&](int p) {
-        const bool pok = p >= 0 && p < nx;
-        rm = 0;
-        if (pok && own_ok) {
-            const long long n = (long long)ko + (long long)nz * (p + (long long)nx * jo);
-            if (mask) rm = mask[n];
-#pragma unroll
-            for (int d = 0; d < 3; d++) rv[d] = u[3 * n + d];
-        } else {
-#pragma unroll
-            for (int d = 0; d < 3; d++) rv[d] = T(0);
-        }
-        if (w == TY) {
-            rxm = 0;
-            if (pok && ext_ok) {
-                const long long n = (long long)ko + (long long)nz * (p + (long long)nx * jx);
-                if (mask) rxm = mask[n];
-#pragma unroll
-                for (int d = 0; d < 3; d++) rx[d] = u[3 * n + d];
-            } else {
-#pragma unroll
-                for (int d = 0; d < 3; d++) rx[d] = T(0);
-            }
-        }
-    };
-    [[maybe_unused]] auto publish = [&](int buf) {
-#pragma unroll
-        for (int d = 0; d < 3; d++) s_u[buf][d][w][l] = ((rm >> d) & 1) ? T(0) : rv[d];
-        if (w == TY) {
-#pragma unroll
-            for (int d = 0; d < 3; d++) s_u[buf][d][TY + 1][l] = ((rxm >> d) & 1) ? T(0) : rx[d];
-        }
-    };
-    auto face = [&](int buf, T g[3][2][2]) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const T f00 = s_u[buf][c][w][l], f01 = s_u[buf][c][w][l + 1];
-            const T f10 = s_u[buf][c][w + 1][l], f11 = s_u[buf][c][w + 1][l + 1];
-            const T s0 = f00 + f10, s1 = f01 + f11, d0 = f10 - f00, d1 = f11 - f01;
-            g[c][0][0] = s0 + s1;
-            g[c][0][1] = s1 - s0;
-            g[c][1][0] = d0 + d1;
-            g[c][1][1] = d1 - d0;
-        }
-    };
-    auto epi_copy = [&](int slot, const T* src, long long n) {
-#pragma unroll
-        for (int d = 0; d < 3; d++) cp_async(&s_ep[slot][d][tid], src + 3 * n + d, TB_);
-    };
-
-    if (CM == 0 && tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
-    // the coefficients are re-read from shared memory at every use (volatile) rather than
-    // held in 72 (FP32) / 144 (FP64) registers for the whole kernel
-    const volatile T* vb = s_blk;
-#define BK(p, i, j) vb[(p) * 9 + (i) * 3 + (j)]
-    // cube element: diagonal minus off-diagonal of the two circulant class blocks
-    [[maybe_unused]] const T amb = cf.c[0] - cf.c[1], fmg = cf.c[5] - cf.c[6];
-    // prologue: planes ix0-1 (buffer 0) and ix0 (buffer 1); FP32: plane ix0+1 in flight
-    [[maybe_unused]] uint8_t mq[NQ];
-    if constexpr (RS) {
-        if (tid < 2 * 3 * PR) (&s_u[0][0][0][0])[tid * PC + 32] = T(0);
-        load_plane(ix0 - 1);
-        publish(0);
-        load_plane(ix0);
-        publish(1);
-        load_plane(ix0 + 1);
-    } else {
-        issue_plane(ix0 - 1, 0, mq);
-        cp_async_commit();
-        cp_async_wait_all();
-        fix_plane(0, mq);
-        issue_plane(ix0, 1, mq);
-        cp_async_commit();
-        cp_async_wait_all();
-        fix_plane(1, mq);
-    }
-    __syncthreads();
-    T glo[3][2][2], carry[3][2][2];
-    face(0, glo);
-    __syncthreads();  // step 0 refills buffer 0: every warp must have read it first
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int b = 0; b < 2; b++) carry[c][a][b] = T(0);
-    T e_next = T(0);
-    if (col_ok && ix0 - 1 >= 0 && ix0 - 1 < NX) e_next = (T)E[((long long)(ix0 - 1) * NY + je) * NZ + ke];
-
-    for (int s = 0; s <= CXc; s++) {
-        const int ie = ix0 - 1 + s;
-        const int cur = (s + 1) & 1;
-        // 1. asynchronous copies (FP64: plane ie+2 into buffer s&1) and epilogue operands
-        if constexpr (!RS) issue_plane(ie + 2, s & 1, mq);
-        const bool out_now = owner && s >= 1 && ie < nx;
-        long long n_out = 0;
-        uint8_t m_out = 0;
-        if (out_now) {
-            n_out = (long long)kn + (long long)nz * (ie + (long long)nx * jn);
-            m_out = mask ? mask[n_out] : (uint8_t)0;
-            if (m_out) epi_copy(0, u, n_out);
-            if constexpr (need_b) epi_copy(1, epi.b, n_out);
-            if constexpr (mode == PF_EPI_JACOBI || need_xa) epi_copy(2, epi.x, n_out);
-            if constexpr (need_d) epi_copy(3, epi.dinv, n_out);
-            if constexpr (need_xa) epi_copy(4, epi.xadd, n_out);
-            if constexpr (need_dot) epi_copy(5, epi.dot_a, n_out);
-        }
-        cp_async_commit();
-        const T e = e_next;
-        e_next = (col_ok && ie + 1 >= 0 && ie + 1 < NX) ? (T)E[((long long)(ie + 1) * NY + je) * NZ + ke] : T(0);
-        // 2. element operator
-        T ghi[3][2][2];
-        face(cur, ghi);
-        // Element operator by (y,z) parity: the pair of classes p = (0,py,pz), (1,py,pz)
-        // reads and writes exactly the modes (c=0: py,pz), (c=1: py^1,pz), (c=2: py,pz^1),
-        // so x stage, two 3x3 blocks and the inverse x stage complete per pair.
-        T G[3][2][2];
-        if constexpr (CM == 0) {
-    #pragma unroll
-            for (int pyz = 0; pyz < 4; pyz++) {
-                const int py = pyz & 1, pz = pyz >> 1;
-                const int p0 = 2 * py + 4 * pz, p1 = p0 + 1;
-                // x stage of the three (component, y-mode, z-mode) slots of this pair
-                const T h0 = e * ghi[0][py][pz], h1 = e * ghi[1][py ^ 1][pz], h2 = e * ghi[2][py][pz ^ 1];
-                const T a0 = fma(e, glo[0][py][pz], h0), b0 = fma(-e, glo[0][py][pz], h0);
-                const T a1 = fma(e, glo[1][py ^ 1][pz], h1), b1 = fma(-e, glo[1][py ^ 1][pz], h1);
-                const T a2 = fma(e, glo[2][py][pz ^ 1], h2), b2 = fma(-e, glo[2][py][pz ^ 1], h2);
-                // class p0 (px = 0): comp 0 in x-mode 1, comps 1, 2 in x-mode 0
-                const T o00 = fma(BK(p0, 0, 0), b0, fma(BK(p0, 0, 1), a1, BK(p0, 0, 2) * a2));
-                const T o01 = fma(BK(p0, 1, 0), b0, fma(BK(p0, 1, 1), a1, BK(p0, 1, 2) * a2));
-                const T o02 = fma(BK(p0, 2, 0), b0, fma(BK(p0, 2, 1), a1, BK(p0, 2, 2) * a2));
-                // class p1 (px = 1): comp 0 in x-mode 0, comps 1, 2 in x-mode 1
-                const T o10 = fma(BK(p1, 0, 0), a0, fma(BK(p1, 0, 1), b1, BK(p1, 0, 2) * b2));
-                const T o11 = fma(BK(p1, 1, 0), a0, fma(BK(p1, 1, 1), b1, BK(p1, 1, 2) * b2));
-                const T o12 = fma(BK(p1, 2, 0), a0, fma(BK(p1, 2, 1), b1, BK(p1, 2, 2) * b2));
-                // inverse x stage: (x-mode 0, x-mode 1) -> lower face w0 - w1, upper face w0 + w1
-                G[0][py][pz] = (o10 - o00) + carry[0][py][pz];
-                carry[0][py][pz] = o10 + o00;
-                G[1][py ^ 1][pz] = (o01 - o11) + carry[1][py ^ 1][pz];
-                carry[1][py ^ 1][pz] = o01 + o11;
-                G[2][py][pz ^ 1] = (o02 - o12) + carry[2][py][pz ^ 1];
-                carry[2][py][pz ^ 1] = o02 + o12;
-            }
-        } else {
-#define KC(q) coef<q, CM, T>(cf)
-            // x stage of slot (component c, y-mode ym, z-mode zm): a = x-mode 0, b = x-mode 1
-#define XST(c, ym, zm, A, B)                          \
-    const T A = e * (ghi[c][ym][zm] + glo[c][ym][zm]); \
-    const T B = e * (ghi[c][ym][zm] - glo[c][ym][zm]);
-            // inverse x stage for pair (py, pz): classes p0 (outputs o0*) and p1 (o1*)
-#define XINV(py, pz, o00, o01, o02, o10, o11, o12)                  \
-    G[0][py][pz] = ((o10) - (o00)) + carry[0][py][pz];              \
-    carry[0][py][pz] = (o10) + (o00);                               \
-    G[1][(py) ^ 1][pz] = ((o01) - (o11)) + carry[1][(py) ^ 1][pz];  \
-    carry[1][(py) ^ 1][pz] = (o01) + (o11);                         \
-    G[2][py][(pz) ^ 1] = ((o02) - (o12)) + carry[2][py][(pz) ^ 1];  \
-    carry[2][py][(pz) ^ 1] = (o02) + (o12);
-            {  // pair (0,0): class 0 full, class 1 on components 1, 2
-                XST(0, 0, 0, a0, b0)
-                XST(1, 1, 0, a1, b1)
-                XST(2, 0, 1, a2, b2)
-                (void)a0;
-                T o00, o01, o02;
-                if constexpr (CM == 2) {  // cube: [[a,b,b],[b,a,b],[b,b,a]] v = (a - b) v + b sum(v)
-                    const T bs = KC(1) * (b0 + a1 + a2);
-                    o00 = fma(amb, b0, bs);
-                    o01 = fma(amb, a1, bs);
-                    o02 = fma(amb, a2, bs);
-                } else {
-                    o00 = fma(KC(0), b0, fma(KC(1), a1, KC(2) * a2));
-                    o01 = fma(KC(1), b0, fma(KC(3), a1, KC(4) * a2));
-                    o02 = fma(KC(2), b0, fma(KC(4), a1, KC(5) * a2));
-                }
-                const T o11 = fma(KC(6), b1, KC(7) * b2);
-                const T o12 = fma(KC(7), b1, KC(8) * b2);
-                XINV(0, 0, o00, o01, o02, T(0), o11, o12)
-            }
-            {  // pair (1,0): class 2 on components 0, 2; class 3 on 0, 1 and 2 alone
-                XST(0, 1, 0, a0, b0)
-                XST(1, 0, 0, a1, b1)
-                XST(2, 1, 1, a2, b2)
-                (void)a1;
-                const T o00 = fma(KC(9), b0, KC(10) * a2);
-                const T o02 = fma(KC(10), b0, KC(11) * a2);
-                T o10, o11;
-                if constexpr (CM == 2) {  // cube: [[d,d],[d,d]]
-                    o10 = KC(12) * (a0 + b1);
-                    o11 = o10;
-                } else {
-                    o10 = fma(KC(12), a0, KC(13) * b1);
-                    o11 = fma(KC(13), a0, KC(14) * b1);
-                }
-                const T o12 = KC(15) * b2;
-                XINV(1, 0, o00, T(0), o02, o10, o11, o12)
-            }
-            {  // pair (0,1): class 4 on components 0, 1; class 5 on 0, 2 and 1 alone
-                XST(0, 0, 1, a0, b0)
-                XST(1, 1, 1, a1, b1)
-                XST(2, 0, 0, a2, b2)
-                (void)a2;
-                const T o00 = fma(KC(16), b0, KC(17) * a1);
-                const T o01 = fma(KC(17), b0, KC(18) * a1);
-                T o10, o12;
-                if constexpr (CM == 2) {  // cube: components 0, 2 coupled by [[d,d],[d,d]]
-                    o10 = KC(19) * (a0 + b2);
-                    o12 = o10;
-                } else {
-                    o10 = fma(KC(19), a0, KC(20) * b2);
-                    o12 = fma(KC(20), a0, KC(21) * b2);
-                }
-                const T o11 = KC(22) * b1;
-                XINV(0, 1, o00, o01, T(0), o10, o11, o12)
-            }
-            {  // pair (1,1): class 6 on 0 alone and 1, 2; class 7 full
-                XST(0, 1, 1, a0, b0)
-                XST(1, 0, 1, a1, b1)
-                XST(2, 1, 0, a2, b2)
-                const T o00 = KC(26) * b0;
-                T o01, o02, o10, o11, o12;
-                if constexpr (CM == 2) {  // cube: class 6 [[d,d],[d,d]] on 1, 2; class 7 circulant
-                    o01 = KC(23) * (a1 + a2);
-                    o02 = o01;
-                    const T gs = KC(28) * (a0 + b1 + b2);
-                    o10 = fma(fmg, a0, gs);
-                    o11 = fma(fmg, b1, gs);
-                    o12 = fma(fmg, b2, gs);
-                } else {
-                    o01 = fma(KC(23), a1, KC(24) * a2);
-                    o02 = fma(KC(24), a1, KC(25) * a2);
-                    o10 = fma(KC(27), a0, fma(KC(28), b1, KC(29) * b2));
-                    o11 = fma(KC(28), a0, fma(KC(30), b1, KC(31) * b2));
-                    o12 = fma(KC(29), a0, fma(KC(31), b1, KC(32) * b2));
-                }
-                XINV(1, 1, o00, o01, o02, o10, o11, o12)
-            }
-#undef XINV
-#undef XST
-#undef KC
-        }
-        // inverse z then y stage -> corner contributions t[c][b][cz]
-        T t[3][2][2];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const T q00 = G[c][0][0] - G[c][0][1], q01 = G[c][0][0] + G[c][0][1];
-            const T q10 = G[c][1][0] - G[c][1][1], q11 = G[c][1][0] + G[c][1][1];
-            t[c][0][0] = q00 - q10;
-            t[c][0][1] = q01 - q11;
-            t[c][1][0] = q00 + q10;
-            t[c][1][1] = q01 + q11;
-        }
-        // node (je+1, ke+1) = t_own[1][1] + t_{l+1}[1][0] + t_{w+1}[0][1] + t_{w+1,l+1}[0][0]
-        T P1[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            P1[c] = t[c][1][1] + __shfl_down_sync(0xffffffffu, t[c][1][0], 1);
-            const T P0 = t[c][0][1] + __shfl_down_sync(0xffffffffu, t[c][0][0], 1);
-            s_x[s & 1][c][w][l] = P0;
-        }
-        // 3. FP32: publish plane ie+2 (loaded during the previous step), load plane ie+3;
-        //    FP64: zero the constrained components of the copied plane; one barrier
-        if constexpr (RS) {
-            publish(s & 1);
-            load_plane(ie + 3);
-            cp_async_wait_all();
-        } else {
-            cp_async_wait_all();
-            fix_plane(s & 1, mq);
-        }
-        __syncthreads();
-        // 4. owners finish their node of plane ie
-        if (out_now) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                T y = P1[c] + s_x[s & 1][c][w + 1][l];
-                if (m_out & (1 << c)) y = s_ep[0][c][tid];
-                T o = y;
-                if constexpr (mode == PF_EPI_RESID) {
-                    o = s_ep[1][c][tid] - y;
-                } else if constexpr (mode == PF_EPI_JACOBI) {
-                    o = s_ep[2][c][tid] + wgt * s_ep[3][c][tid] * (s_ep[1][c][tid] - y);
-                } else if constexpr (mode == PF_EPI_JACOBI_ADD) {
-                    o = s_ep[4][c][tid] + s_ep[2][c][tid] + wgt * s_ep[3][c][tid] * (s_ep[1][c][tid] - y);
-                }
-                epi.out[3 * n_out + c] = o;
-                if constexpr (need_dot) dot += (double)s_ep[5][c][tid] * (double)(epi.dot_of_y ? y : o);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int a = 0; a < 2; a++)
-#pragma unroll
-                for (int b = 0; b < 2; b++) glo[c][a][b] = ghi[c][a][b];
-    }
-#undef BK
-    if constexpr (DOT) {
-        const double sblk = block_sum<NT>(dot, s_red);
-        if (threadIdx.x == 0)
-            epi.dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = sblk;
-    }
-}
 
 // ---------------------------------------------------------------------------------------
 // 3D matvec: register x-march
@@ -896,29 +483,10 @@ static H8Blk<T> make_blk(const Op* op) {
     return b;
 }
 
-constexpr int kTY64 = 4;  // FP64: 5 warps per block
-constexpr int kTY32 = 8;  // FP32: 9 warps per block
-
-static void h8_launch_dims(const Grid& g, int TY, bool fp32, dim3* grid, int* CXc) {
-    const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
-    const int zt = fp32 ? kZTile32 : kZTile64;
-    const int tz = (nz + zt - 1) / zt, ty = (ny + TY - 1) / TY;
-    // enough x-chunks for ~4 waves of blocks, chunks of 4..32 planes
-    const long long target = 4LL * kNumSM * 3;
-    int chunks = (int)((target + (long long)tz * ty - 1) / ((long long)tz * ty));
-    int cx = (nx + chunks - 1) / chunks;
-    cx = cx < 4 ? 4 : (cx > 32 ? 32 : cx);
-    *CXc = cx;
-    *grid = dim3(tz, ty, (nx + cx - 1) / cx);
-}
-
 // register x-march: NW warps per block (NW - 1 owned node rows), at least MINB blocks per SM
 // (FP64: 8 warps x 2 blocks, up to 128 registers; FP32: 12 warps x 2 blocks, up to 80;
 // FP32 with 9 warps x 3 blocks at 72 registers measured slower)
 constexpr int kNWr64 = 8, kMinBr64 = 2, kNWr32 = 12, kMinBr32 = 2;
-
-// the register x-march indexes nodes in 32 bits
-static bool h8r_fits(const Grid& g) { return 3LL * g.n_nodes < (1LL << 31) && g.n_elem < (1LL << 31); }
 
 // x-chunk length: fewest estimated block-steps, counting whole waves of the resident slots
 // (ties go to the longer chunk, which recomputes fewer boundary elements)
@@ -945,10 +513,7 @@ static void h8r_launch_dims(const Grid& g, bool fp32, dim3* grid, int* CXc) {
 long long h8_num_blocks(const Grid& g, int fp32) {
     dim3 gr;
     int cx;
-    if (h8r_fits(g))
-        h8r_launch_dims(g, fp32 != 0, &gr, &cx);
-    else
-        h8_launch_dims(g, fp32 ? kTY32 : kTY64, fp32 != 0, &gr, &cx);
+    h8r_launch_dims(g, fp32 != 0, &gr, &cx);
     return (long long)gr.x * gr.y * gr.z;
 }
 
@@ -1021,14 +586,6 @@ long long q4_num_blocks(const Grid& g) { return (g.n_nodes + 255) / 256; }
 // ---------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------
-template <typename T, typename TE, int TY, int CM, int MODE, bool DOT>
-static int h8_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
-                     const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, cudaStream_t st) {
-    PF_CUDA(launch_pdl(k_matvec_h8<T, TE, TY, CM, MODE, DOT>, dim3(grid), dim3((TY + 1) * 32), 0, st, g.nel[0], g.nel[1],
-                       g.nel[2], cx, u, E, mask, blk, cf, epi));
-    return PF_OK;
-}
-
 template <typename T, typename TE, int CM, int MODE, bool DOT>
 static int h8r_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
                       const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, cudaStream_t st) {
@@ -1038,6 +595,7 @@ static int h8r_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E,
     return PF_OK;
 }
 
+// the epilogue mode and the fused dot are template parameters of the kernel
 template <typename T, typename TE, int CM>
 static int h8r_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
                         const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, bool dot, cudaStream_t st) {
@@ -1059,83 +617,37 @@ static int h8r_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* 
 #undef PF_H8R
 }
 
-template <typename T, typename TE, int TY, int CM>
-static int h8_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
-                       const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, bool dot, cudaStream_t st) {
-#define PF_H8(M, D) return h8_launch<T, TE, TY, CM, M, D>(grid, cx, g, u, E, mask, blk, cf, epi, st)
-    switch (epi.mode) {
-        case PF_EPI_STORE:
-            if (dot) PF_H8(PF_EPI_STORE, true);
-            PF_H8(PF_EPI_STORE, false);
-        case PF_EPI_RESID:
-            if (dot) PF_H8(PF_EPI_RESID, true);
-            PF_H8(PF_EPI_RESID, false);
-        case PF_EPI_JACOBI:
-            if (dot) PF_H8(PF_EPI_JACOBI, true);
-            PF_H8(PF_EPI_JACOBI, false);
-        default:
-            if (dot) PF_H8(PF_EPI_JACOBI_ADD, true);
-            PF_H8(PF_EPI_JACOBI_ADD, false);
-    }
-#undef PF_H8
-}
-
 template <typename T, typename TE>
 int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mask, const Epi<T>& epi,
                        cudaStream_t st) {
     const Grid& g = op->grid;
     if (g.dim == 3) {
-        constexpr int TY = sizeof(T) == 8 ? kTY64 : kTY32;
-        dim3 grid;
-        int cx;
-        h8_launch_dims(g, TY, sizeof(T) == 4, &grid, &cx);
-        // FP32, isotropic box elements: the 33 nonzero coefficients (read as constant
-        // operands); FP64: the 7 values of a cube element in registers, other boxes the
-        // dense blocks from shared memory (33 double registers would cut the occupancy)
-        const int cm = sizeof(T) == 4 ? (op->sparse ? 1 : 0) : (op->cube ? 2 : 0);
+        // a cube element's seven values (a-b, b, c, d, e, f-g, g), the 33 nonzeros of another
+        // isotropic box, or (CM 0) the dense class blocks
+        const int cm = op->cube ? 2 : (op->sparse ? 1 : 0);
         H8Coef<T> cf;
         for (int q = 0; q < 33; q++) cf.c[q] = T(0);
-        if (cm == 1)
+        if (cm == 2) {
+            const double* v = op->cube_v;
+            const double vals[7] = {v[0] - v[1], v[1], v[2], v[3], v[4], v[5] - v[6], v[6]};
+            for (int q = 0; q < 7; q++) cf.c[q] = (T)vals[q];
+        } else if (cm == 1) {
             for (int q = 0; q < 33; q++) cf.c[q] = (T)op->coef[q];
-        if (cm == 2)
-            for (int v = 0; v < 7; v++) cf.c[v] = (T)op->cube_v[v];
-        const H8Blk<T> blk = make_blk<T>(op);
-        pf::count_launch();
-        if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");
-        if (h8r_fits(g)) {
-            // register x-march: a cube element's seven values (a-b, b, c, d, e, f-g, g), the
-            // 33 nonzeros of another isotropic box, or the dense blocks
-            const int cmr = op->cube ? 2 : (op->sparse ? 1 : 0);
-            H8Coef<T> cr;
-            for (int q = 0; q < 33; q++) cr.c[q] = T(0);
-            if (cmr == 2) {
-                const double* v = op->cube_v;
-                const double vals[7] = {v[0] - v[1], v[1], v[2], v[3], v[4], v[5] - v[6], v[6]};
-                for (int q = 0; q < 7; q++) cr.c[q] = (T)vals[q];
-            } else if (cmr == 1) {
-                for (int q = 0; q < 33; q++) cr.c[q] = (T)op->coef[q];
-            }
-            h8r_launch_dims(g, sizeof(T) == 4, &grid, &cx);
-            const bool dot = epi.dot_partial != nullptr;
-            int s;
-            if (cmr == 2)
-                s = h8r_dispatch<T, TE, 2>(grid, cx, g, u, E, mask, blk, cr, epi, dot, st);
-            else if (cmr == 1)
-                s = h8r_dispatch<T, TE, 1>(grid, cx, g, u, E, mask, blk, cr, epi, dot, st);
-            else
-                s = h8r_dispatch<T, TE, 0>(grid, cx, g, u, E, mask, blk, cr, epi, dot, st);
-            if (s) return s;
-            PF_LAUNCH_CHECK("fine matvec launch");
-            return PF_OK;
         }
-        constexpr int CMS = sizeof(T) == 4 ? 1 : 2;  // the sparse variant of this precision
-        const bool dot = epi.dot_partial != nullptr;
+        const H8Blk<T> blk = make_blk<T>(op);
         if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");
+        dim3 grid;
+        int cx;
+        h8r_launch_dims(g, sizeof(T) == 4, &grid, &cx);
+        pf::count_launch();
+        const bool dot = epi.dot_partial != nullptr;
         int s;
-        if (cm != 0)
-            s = h8_dispatch<T, TE, TY, CMS>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+        if (cm == 2)
+            s = h8r_dispatch<T, TE, 2>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+        else if (cm == 1)
+            s = h8r_dispatch<T, TE, 1>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
         else
-            s = h8_dispatch<T, TE, TY, 0>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+            s = h8r_dispatch<T, TE, 0>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
         if (s) return s;
     } else {
         const long long nb = q4_num_blocks(g);
