@@ -198,9 +198,12 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_alpha(const double* partial
     }
 }
 
+// x += alpha p, r -= alpha q, partial sums of r.r; with rf (mixed form) also the FP32 copy
+// of r that the V-cycle reads
 __global__ void __launch_bounds__(kRedThreads) k_pcg_xr(long long n, const double* __restrict__ p,
                                                         const double* __restrict__ q, double* __restrict__ x,
-                                                        double* __restrict__ r, const PcgState* st, double* partials) {
+                                                        double* __restrict__ r, const PcgState* st, double* partials,
+                                                        float* __restrict__ rf) {
     pdl_wait();
     pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
@@ -211,6 +214,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_xr(long long n, const doubl
         x[i] += a * p[i];
         const double ri = r[i] - a * q[i];
         r[i] = ri;
+        if (rf) rf[i] = (float)ri;
         s += ri * ri;
     }
     s = block_sum<kRedThreads>(s, s_red);
@@ -666,12 +670,16 @@ extern "C" int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega,
 }
 
 // apply the preconditioner to mg->r, leave r.z partials in mg->partials and return z
-static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaStream_t st) {
+// (mixed form: r32_ready = the FP32 copy of r is already in the V-cycle's input)
+static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaStream_t st, bool r32_ready) {
     const long long n = mg->L[0].ndof;
     int s;
     if (mg->fp32) {
-        pf::count_launch();
-        PF_CUDA(launch_pdl(k_d2f_skip, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, (float*)mg->L[0].b, &mg->st->done));
+        if (!r32_ready) {
+            pf::count_launch();
+            PF_CUDA(launch_pdl(k_d2f_skip, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, (float*)mg->L[0].b,
+                               &mg->st->done));
+        }
         float* res;
         if ((s = vcycle<float>(mg, 0, (const float*)mg->L[0].b, &res, nullptr, nullptr, st))) return s;
         pf::count_launch();
@@ -712,13 +720,14 @@ static int pcg_iteration(pf_mg* mg, double* x, cudaStream_t st) {
     pf::count_launch();
     PF_CUDA(launch_pdl(k_pcg_alpha, dim3(1), dim3(kRedThreads), 0, st, mg->partials, fine_matvec_num_blocks(mg->op, 0), mg->st));
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_pcg_xr, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->p, mg->q, x, mg->r, mg->st, mg->partials));
+    PF_CUDA(launch_pdl(k_pcg_xr, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->p, mg->q, x, mg->r, mg->st, mg->partials,
+                       mg->fp32 ? (float*)mg->L[0].b : (float*)nullptr));
     pf::count_launch();
     PF_CUDA(launch_pdl(k_pcg_check, dim3(1), dim3(kRedThreads), 0, st, mg->partials, vec_blocks(n), mg->st));
     PF_LAUNCH_CHECK("pcg launch");
     const void* z;
     long long np;
-    if ((s = precondition(mg, &z, &np, st))) return s;
+    if ((s = precondition(mg, &z, &np, st, true))) return s;
     pf::count_launch();
     PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st));
     PF_LAUNCH_CHECK("beta launch");
@@ -764,7 +773,7 @@ static int solve_start(pf_mg* mg, int use_x0, cudaStream_t st) {
     PF_LAUNCH_CHECK("pcg start");
     const void* z;
     long long np;
-    if ((s = precondition(mg, &z, &np, st))) return s;
+    if ((s = precondition(mg, &z, &np, st, false))) return s;
     pf::count_launch();
     PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st));
     return update_p(mg, z, 1, st);
@@ -934,7 +943,7 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
             pf::count_launch();
             PF_CUDA(launch_pdl(k_pcg_alpha, dim3(1), dim3(kRedThreads), 0, st, partials, nbm, S));
             pf::count_launch();
-            PF_CUDA(launch_pdl(k_pcg_xr, dim3(vb), dim3(kRedThreads), 0, st, n, p, q, x, r, S, partials));
+            PF_CUDA(launch_pdl(k_pcg_xr, dim3(vb), dim3(kRedThreads), 0, st, n, p, q, x, r, S, partials, (float*)nullptr));
             pf::count_launch();
             PF_CUDA(launch_pdl(k_pcg_check, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
             pf::count_launch();

@@ -110,6 +110,22 @@ def test_matvec_vs_oracle_shapes(lib, nel):
     assert rel(y32, O.matvec(nel, K0, E.astype(np.float32), u.astype(np.float32), cons)) < 2e-5
 
 
+@pytest.mark.parametrize("nel", [(3, 6, 29), (5, 13, 30), (70, 11, 59), (9, 22, 89), (130, 3, 3), (4, 12, 1)])
+def test_matvec_march_tile_edges(lib, nel):
+    """The x-march's own tiling: 30 owned node columns per warp (nz = 30, 31, 60, 90), 7
+    (FP64) and 11 (FP32) owned node rows per block (ny = 7, 12, 14, 23), and x chunks of
+    whatever length the wave model picks (nx = 4 .. 131), with constraints on a tenth of the
+    DOFs, FP64 and FP32 against the oracle."""
+    rng = np.random.default_rng(sum(nel) + 7)
+    op = Op(lib, nel)
+    E = rng.uniform(1e-3, 1.0, int(np.prod(nel)))
+    u = rng.standard_normal(op.ndof)
+    cons = rng.choice(op.ndof, size=max(1, op.ndof // 10), replace=False)
+    assert rel(op.matvec(E, u, cons), O.matvec(nel, op.K0, E, u, cons)) < 1e-12
+    E32, u32 = E.astype(np.float32), u.astype(np.float32)
+    assert rel(op.matvec(E32, u32, cons, fp32=True), O.matvec(nel, op.K0, E32, u32, cons)) < 2e-5
+
+
 @pytest.mark.parametrize("nel", [(96, 48, 48), (64, 64, 64), (48, 96, 40)])
 def test_matvec_large_and_repeatable(lib, nel):
     """Full-size grids (many blocks per SM, every tile and chunk edge) in FP64 and FP32, and
