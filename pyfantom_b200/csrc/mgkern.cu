@@ -204,9 +204,11 @@ template int launch_prolong<float>(const Grid&, const float*, float*, const int*
 // each tile's (NB+1)/2 * DIM^2 coefficient rows are one contiguous run (16 KB in 3D FP32),
 // so DRAM streams through it instead of jumping between NH*BS planes of N values.
 // ---------------------------------------------------------------------------------------
+// Launch bounds: FP32 keeps 7 blocks per SM (32 registers); FP64 lets the compiler take 56
+// registers (4 blocks per SM), measured faster than its default 40 for the FP64 solves.
 template <int DIM, typename T, bool HALF>
-__global__ void __launch_bounds__(DIM == 3 ? 288 : 96) k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A,
-                                                                        const T* __restrict__ u, Epi<T> epi) {
+__global__ void __launch_bounds__(DIM == 3 ? 288 : 96, (DIM == 3 && sizeof(T) == 4) ? 7 : 1)
+    k_stencil_matvec(GridDev<DIM> g, const T* __restrict__ A, const T* __restrict__ u, Epi<T> epi) {
     pdl_wait();
     pdl_trigger();
     constexpr int NB = DIM == 3 ? 27 : 9, BS = DIM * DIM, NG = NB / 3, C = NB / 2;
