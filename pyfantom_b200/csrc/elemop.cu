@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     const bool ok0 = col_ok && je >= 0 && je < ny, ok1 = col_ok && je + 1 < ny;
     const bool elem_ok = l < 31 && je >= 0 && je < NY && kc >= 0 && kc < NZ;
     const bool owner = w < TY && l < kZTileR && je + 1 < ny && kc + 1 < nz;
-    // 32-bit node and element indices (the launcher checks 3 * nodes < 2^31)
+    // 32-bit node and element indices (grid validation keeps 3 * nodes below 2^31)
     const int rows = nz * nx;        // nodes per node row (y)
     const int n0 = kc + rows * je;   // node (je, 0, kc): rows je, je + 1 advance by nz per plane
     const int n1 = n0 + rows;
