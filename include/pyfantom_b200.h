@@ -292,13 +292,19 @@ int pf_pgd_project_f64(long long n, const double* xs, const double* dg, double v
 
 /* ---- OC update without allocation --------------------------------------------------
  * No counterpart in the reference.  Same computation and outputs as pf_oc_update_f64,
- * for callers that cannot allocate device memory where they run the OC step (code being
- * captured into a CUDA graph, plugins inside a framework that owns the device memory,
- * latency-bound per-iteration callbacks): the scratch is a static device array of the
- * library sized for PF_OC_NOALLOC_MAX_ELEMS elements (16.9 MB held by every GPU that loads
- * the library).  Larger n is rejected with PF_BAD_ARG.  The first call on each device
- * resolves the array's address (and may load the library's device code): make it before
- * any stream capture.  Calls share the array: calls that overlap on the GPU race. */
+ * for callers that cannot allocate device memory where they run the OC step: plugins
+ * inside a framework that owns the device memory (its caching allocator may hold nearly
+ * all of it, and the plugin must not allocate behind its back) and per-iteration
+ * callbacks with a latency budget (cudaMalloc synchronises the device).  The scratch is
+ * a static device array of the library sized for PF_OC_NOALLOC_MAX_ELEMS elements
+ * (16.9 MB held by every GPU that loads the library until the process exits).  Larger n
+ * is rejected with PF_BAD_ARG.  The first call on each device resolves the array's
+ * address with that device current and keeps it (it may also load the library's device
+ * code), so that first call should come before any stream capture; after a
+ * cudaDeviceReset the kept address is stale and the entry point must not be called
+ * again in that process.  A non-NULL h_out makes the call wait for the stream to deliver
+ * {||x_new - x||, lambda, steps}; pass NULL where the caller must not wait.  Calls share
+ * the array: calls that overlap on the GPU race. */
 #define PF_OC_NOALLOC_MAX_ELEMS 2097152
 int pf_oc_update_noalloc_f64(long long n, const double* x, const double* df, const double* dg, double vf,
                              double move, double* x_new, double* h_out, void* stream);

@@ -103,7 +103,9 @@ class OC(Optimizer):
         if self.timer:
             end = time.time()
         p.set_desvars(x_new)
-        self.change = float(torch.linalg.norm(self.last_desvars - x_new))
+        # ||x_new - x|| from the update kernel: x is the design the previous iteration set
+        # (the reference takes ||last_desvars - desvars_new||, OC.py:137)
+        self.change = change
         f = p.f()
         self.change_f = float(torch.abs((f - self.last_f) / f))
         self.last_f = f

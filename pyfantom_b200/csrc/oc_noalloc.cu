@@ -1,22 +1,24 @@
 // OC update that allocates nothing: the scratch lives in a static device array.
 //
 // Who needs this: callers that cannot call cudaMalloc on the path where they run the OC
-// step - code being recorded into a CUDA graph by stream capture (cudaMalloc is not a
-// stream operation and breaks or is forbidden during capture), plugins hosted by a
-// framework that owns the device memory (its caching allocator may hold nearly all of it,
-// and the plugin must not allocate behind its back), and per-iteration callbacks with a
-// latency budget, where a device allocation (which synchronises) is not acceptable.  The
-// regular pf_oc_update_f64 asks such callers for a workspace they cannot provide.
+// step - plugins hosted by a framework that owns the device memory (its caching allocator
+// may hold nearly all of it, and the plugin must not allocate behind its back), and
+// per-iteration callbacks with a latency budget, where a device allocation (which
+// synchronises the device) is not acceptable.  The regular pf_oc_update_f64 asks such
+// callers for a workspace they cannot provide.
 //
 // The scratch is a file-scope __device__ array sized for PF_OC_NOALLOC_MAX_ELEMS
 // elements (16.9 MB); every GPU that loads this library holds it until the process exits.
 // Host code cannot use the array's name as a device address, so the first call on each
-// device resolves it with cudaGetSymbolAddress while that device is current and caches
+// device resolves it with cudaGetSymbolAddress while that device is current and keeps
 // the pointer.  That first call may also load the library's device code, so it should
-// come before any stream capture.  All calls share the array and it keeps the contents
-// of the last call; the kernels initialise every value they read (the bisection state
-// and all partial sums are written before use), so nothing needs clearing between calls.
-// Calls that overlap on the GPU (different streams without ordering) race on the array.
+// come before any stream capture.  A cudaDeviceReset invalidates the kept pointer: the
+// entry point must not be called again in that process.  All calls share the array and
+// it keeps the contents of the last call; the kernels initialise every value they read
+// (the bisection state and all partial sums are written before use), so nothing needs
+// clearing between calls.  With a non-NULL h_out the call copies the result scalars to
+// the host and waits for the stream.  Calls that overlap on the GPU (different streams
+// without ordering) race on the array.
 #include <mutex>
 
 #include "common.cuh"

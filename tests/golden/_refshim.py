@@ -18,13 +18,21 @@ import sys
 import types
 from unittest.mock import MagicMock
 
-REFERENCE_ROOT = os.environ.get("PYFANTOM_REFERENCE", "/root/reference")
+
+
+def reference_root() -> str:
+    """The reference checkout to import (environment variable ``PYFANTOM_REFERENCE``)."""
+    root = os.environ.get("PYFANTOM_REFERENCE")
+    if not root:
+        raise RuntimeError("set PYFANTOM_REFERENCE to the reference pyFANTOM checkout to generate goldens")
+    return root
 
 
 def install():
     if "pyFANTOM" in sys.modules:
         return
-    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(os.path.dirname(__file__), "..", "..", "_work", "numba_cache"))
+    import tempfile
+    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "pyfantom_ref_numba_cache"))
     import scipy.sparse as sp
     from scipy.sparse.linalg import splu
 
@@ -47,5 +55,6 @@ def install():
     for name in ["matplotlib", "matplotlib.pyplot", "matplotlib.markers", "matplotlib.path",
                  "matplotlib.collections", "matplotlib.colors", "vtk", "k3d"]:
         sys.modules.setdefault(name, MagicMock())
-    if REFERENCE_ROOT not in sys.path:
-        sys.path.insert(0, REFERENCE_ROOT)
+    root = reference_root()
+    if root not in sys.path:
+        sys.path.insert(0, root)

@@ -1,6 +1,6 @@
 """Generate golden fixtures by running the reference pyFANTOM CPU path in this container.
 
-Usage:  python tests/golden/make_golden.py [--big]
+Usage:  PYFANTOM_REFERENCE=<reference checkout> python tests/golden/make_golden.py [--big]
 
 Writes ``tests/golden/*.npz`` (small arrays) and ``tests/golden/known_answers.json``.
 Every array is produced by the reference's own code (numba kernels and Python classes

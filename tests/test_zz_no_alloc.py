@@ -1,8 +1,9 @@
 """GPU: the allocation-free OC entry point against the regular one.
 
 pf_oc_update_noalloc_f64 exists for callers that cannot allocate device memory where they
-run the OC step (stream capture, framework-owned device memory, latency-bound callbacks);
-it takes its scratch from a static device array instead of a caller workspace.  Its
+run the OC step (a plugin under a framework that owns the device memory, a latency-bound
+per-iteration callback where cudaMalloc would synchronise the device); it takes its
+scratch from a static device array instead of a caller workspace.  Its
 results must equal pf_oc_update_f64's on the same inputs, on consecutive calls (the array
 keeps the previous call's contents), and sizes beyond the array must be refused.  This
 file sorts last so that a run stopping at the first failure has run every other test.
