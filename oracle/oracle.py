@@ -57,6 +57,11 @@ def lib():
             "or_mgcg_solve": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, _ip]),
+            "or_mgcg_solve_timed": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                   _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, _ip, _dp]),
+            "or_cg_solve": (ctypes.c_int, [ctypes.c_int, _ip, _dp, _dp, _bp, _dp, _dp, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_int, _dp]),
             "or_mg_vcycle": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, _dp, _dp, _bp, _dp, _dp]),
             "or_filter_normalizer": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp]),
@@ -226,6 +231,44 @@ def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega
                              pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None),
                              ctypes.byref(res), ctypes.byref(st))
     return x, int(it), float(res.value), int(st.value)
+
+
+def mgcg_solve_timed(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega=0.4, omega_boost=1.06,
+                     tol=1e-8, maxiter=1000):
+    """``mgcg_solve`` from x0 = 0 that also returns the wall-clock seconds of the hierarchy
+    setup and of the PCG iterations: (x, iterations, residual, status, setup_s, iterate_s)."""
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ca, pc = _con(con, nd)
+    ra, pr = _d(rhs)
+    x = np.zeros(nd)
+    res = ctypes.c_double(0.0)
+    st = ctypes.c_int(0)
+    t = np.zeros(2)
+    it = lib().or_mgcg_solve_timed(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
+                                   pK, pw, pc, pr, x.ctypes.data_as(_dp), 0, ctypes.byref(res), ctypes.byref(st),
+                                   t.ctypes.data_as(_dp))
+    return x, int(it), float(res.value), int(st.value), float(t[0]), float(t[1])
+
+
+def cg_solve(nel, K0, w, con, rhs, tol=1e-5, maxiter=1000, x0=None):
+    """Unpreconditioned textbook CG (the cupyx ``cg`` the reference CG solver calls,
+    solvers/CUDA/_solvers.py:114-127).  Returns (x, iterations, relative residual)."""
+    dim = len(nel)
+    nd = n_nodes(nel) * dim
+    nel_a, pn = _i(nel)
+    K0a, pK = _d(K0)
+    wa, pw = _d(w)
+    ca, pc = _con(con, nd)
+    ra, pr = _d(rhs)
+    x = np.zeros(nd) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    res = ctypes.c_double(0.0)
+    it = lib().or_cg_solve(dim, pn, pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None), tol, maxiter,
+                           ctypes.byref(res))
+    return x, int(it), float(res.value)
 
 
 def mg_vcycle(nel, K0, w, con, r, n_level=3, n_smooth=2, omega=0.4, omega_boost=1.06):

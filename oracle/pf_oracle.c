@@ -529,10 +529,20 @@ static void vcycle(mg_t* m, int l, double* x, const double* b, double omega) {
     for (long i = 0; i < n; i++) x[i] += e[i];
 }
 
+/* deterministic dot product: 64 fixed chunks summed in order (an OpenMP reduction
+ * combines thread partials in arrival order, which varies from run to run) */
 static double dot(long n, const double* a, const double* b) {
+    enum { NCH = 64 };
+    double part[NCH];
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < NCH; c++) {
+        const long lo = n * c / NCH, hi = n * (c + 1) / NCH;
+        double s = 0.0;
+        for (long i = lo; i < hi; i++) s += a[i] * b[i];
+        part[c] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for reduction(+ : s)
-    for (long i = 0; i < n; i++) s += a[i] * b[i];
+    for (int c = 0; c < NCH; c++) s += part[c];
     return s;
 }
 
@@ -596,12 +606,24 @@ int or_mg_vcycle(int dim, const int* nel, int n_level, int n_smooth, double omeg
 
 /* returns iterations; *res = final recursive relative residual; status 0 ok, 1 not
  * converged, 2 coarse factorization failed */
-int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
-                  double omega_boost, double tol, int maxiter, const double* K0, const double* w,
-                  const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
-                  int* status_out) {
+static double wall_s(void) {
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return 0.0;
+#endif
+}
+
+/* or_mgcg_solve with wall-clock seconds of the hierarchy setup (times_out[0]) and of the
+ * PCG start plus iterations (times_out[1]); times_out may be NULL */
+int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                        double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                        const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
+                        int* status_out, double* times_out) {
     mg_t m;
+    const double t0 = wall_s();
     int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con);
+    const double t1 = wall_s();
     int iters = 0;
     double R = 0.0;
     int status = 0;
@@ -646,9 +668,76 @@ int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double ome
         }
         free(r); free(z); free(p); free(q);
     }
+    if (times_out) {
+        times_out[0] = t1 - t0;
+        times_out[1] = wall_s() - t1;
+    }
     mg_release(&m);
     *res_out = R;
     *status_out = status;
+    return iters;
+}
+
+int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                  double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                  const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
+                  int* status_out) {
+    return or_mgcg_solve_timed(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w,
+                               con, rhs, x, use_x0, res_out, status_out, NULL);
+}
+
+/* ------------------------------------------------------------------------------------
+ * Unpreconditioned CG on the structured operator: the reference CG solver
+ * (solvers/CUDA/_solvers.py:114-127) calls cupyx.scipy.sparse.linalg.cg(kernel, rhs,
+ * x0, tol, maxiter), which is textbook CG with the identity preconditioner:
+ *   r = b - A x; rho = r.r; p = r (first iteration) or r + (rho / rho_prev) p;
+ *   q = A p; alpha = rho / p.q; x += alpha p; r -= alpha q;
+ *   stop when ||r|| <= tol ||b|| (atol = max(0, tol ||b||)) or after maxiter iterations;
+ *   b = 0 returns x = 0.
+ * Returns the iterations; *res_out = ||r|| / ||b|| (recursive residual).
+ * ---------------------------------------------------------------------------------- */
+int or_cg_solve(int dim, const int* nel, const double* K0, const double* w, const uint8_t* con, const double* rhs,
+                double* x, int use_x0, double tol, int maxiter, double* res_out) {
+    grid_t g = mkgrid(dim, nel);
+    const long n = g.n_nodes * dim;
+    double *r = (double*)malloc(sizeof(double) * n), *p = (double*)malloc(sizeof(double) * n);
+    double* q = (double*)malloc(sizeof(double) * n);
+    const double nb = sqrt(dot(n, rhs, rhs));
+    int iters = 0;
+    double R = 0.0;
+    if (nb == 0.0) {
+        memset(x, 0, sizeof(double) * n);
+    } else {
+        if (!use_x0) memset(x, 0, sizeof(double) * n);
+        or_matvec(dim, nel, K0, w, x, con, q);
+        for (long i = 0; i < n; i++) r[i] = rhs[i] - q[i];
+        const double atol = tol * nb;
+        double rho = 0.0, rho_prev = 0.0;
+        for (int it = 0; it < maxiter; it++) {
+            rho_prev = rho;
+            rho = dot(n, r, r);
+            if (it == 0) {
+                memcpy(p, r, sizeof(double) * n);
+            } else {
+                const double beta = rho / rho_prev;
+#pragma omp parallel for
+                for (long i = 0; i < n; i++) p[i] = r[i] + beta * p[i];
+            }
+            or_matvec(dim, nel, K0, w, p, con, q);
+            const double alpha = rho / dot(n, p, q);
+#pragma omp parallel for
+            for (long i = 0; i < n; i++) {
+                x[i] += alpha * p[i];
+                r[i] -= alpha * q[i];
+            }
+            iters = it + 1;
+            const double rn = sqrt(dot(n, r, r));
+            R = rn / nb;
+            if (rn <= atol) break;
+        }
+    }
+    free(r); free(p); free(q);
+    *res_out = R;
     return iters;
 }
 

@@ -36,7 +36,7 @@ from pyFANTOM.geom.CPU._filters import StructuredFilter2D, StructuredFilter3D  #
 from pyFANTOM.stiffness.CPU import StructuredStiffnessKernel  # noqa: E402
 from pyFANTOM.core.CPU._mgm import (apply_restriction, apply_prolongation,  # noqa: E402
                                     get_restricted_l0, get_restricted_l1p)
-from pyFANTOM.solvers.CPU._solvers import MultiGrid, SPSOLVE  # noqa: E402
+from pyFANTOM.solvers.CPU._solvers import MultiGrid, SPSOLVE, cg as ref_cg  # noqa: E402
 from pyFANTOM.FiniteElement.CPU.FiniteElement import FiniteElement  # noqa: E402
 from pyFANTOM.Problem.CPU.MinimumCompliance import MinimumCompliance  # noqa: E402
 from pyFANTOM.Optimizers.CPU.OC import OC  # noqa: E402
@@ -407,6 +407,28 @@ def solve_goldens():
     save("solve16", **out)
 
 
+def cg_goldens():
+    """Textbook CG iterates: the reference's own CG loop (solvers/CPU/_solvers.py:111-139)
+    run from x0 = 0 with rtol = 0 (never stops early), so that after maxiter = N it returns
+    exactly the N-th iterate; the same iterates as cupyx cg, which the CUDA CG solver calls
+    (solvers/CUDA/_solvers.py:114-127), from the same start."""
+    out = {}
+    for tag, wl, n_its in [("3d", workloads.cantilever3d(8, 4, 4, seed=3), (1, 7, 40)),
+                           ("2d", workloads.mbb2d(16, 8), (1, 9, 60))]:
+        _, kern, fe, _ = _simp_setup(wl, lambda m, k: SPSOLVE(k), 1.5, 0.5)
+        kern.set_rho(wl["E"])
+        rhs = np.array(fe.rhs)
+        out[f"{tag}_nel"] = np.array(wl["nel"])
+        out[f"{tag}_E"] = wl["E"]
+        out[f"{tag}_rhs"] = rhs
+        out[f"{tag}_cons"] = np.nonzero(kern.constraints)[0]
+        out[f"{tag}_its"] = np.array(n_its)
+        for n in n_its:
+            x, _ = ref_cg(kern, rhs, x0=np.zeros_like(rhs), rtol=0.0, maxiter=n)
+            out[f"{tag}_x{n}"] = np.array(x)
+    save("cg", **out)
+
+
 def big_solve():
     wl = workloads.cantilever3d(96, 48, 48, seed=0)
     fac = lambda m, k: MultiGrid(m, k, maxiter=1000, tol=1e-8, n_smooth=2, omega=0.6, n_level=4, cycle="V")
@@ -437,6 +459,7 @@ def main():
     penalize_goldens()
     sensitivity_goldens()
     solve_goldens()
+    cg_goldens()
     f = mbb_trajectory()
     pgd_goldens()
     multimaterial_goldens()

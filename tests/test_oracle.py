@@ -193,3 +193,28 @@ def test_penalize_multi_matches_reference(golden, tag, kw):
     E, dE = O.penalize_multi(rho, E_mul, **kw)
     assert rel(E, g[tag + "_E"]) < 1e-14
     assert rel(dE, g[tag + "_dE"]) < 1e-13
+
+
+@pytest.mark.parametrize("tag", ["3d", "2d"])
+def test_cg_iterates_match_reference(golden, tag):
+    """The oracle's textbook CG takes the reference CG loop's steps: after N iterations from
+    x0 = 0 (rtol 0, so neither stops early) the iterates agree."""
+    g = golden("cg")
+    nel = tuple(int(v) for v in g[tag + "_nel"])
+    K0 = unit_K0(len(nel))
+    for n in g[tag + "_its"]:
+        x, it, _ = O.cg_solve(nel, K0, g[tag + "_E"], g[tag + "_cons"], g[tag + "_rhs"], tol=0.0, maxiter=int(n))
+        assert it == int(n)
+        assert rel(x, g[f"{tag}_x{int(n)}"]) < 1e-10
+
+
+def test_cg_stops_at_tolerance_and_solves():
+    """Stopping rule of cupyx cg: the first iterate with ||r|| <= tol ||b||."""
+    wl = workloads.cantilever3d(8, 4, 4)
+    K0 = unit_K0(3)
+    x, it, res = O.cg_solve(wl["nel"], K0, wl["E"], wl["fixed_dofs"], wl["rhs"], tol=1e-9, maxiter=5000)
+    assert res <= 1e-9
+    _, it_prev, res_prev = O.cg_solve(wl["nel"], K0, wl["E"], wl["fixed_dofs"], wl["rhs"], tol=1e-9, maxiter=it - 1)
+    assert res_prev > 1e-9
+    xm, _, _, _ = O.mgcg_solve(wl["nel"], K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=1, tol=1e-12)
+    assert rel(x, xm) < 1e-7
