@@ -32,6 +32,7 @@ struct PcgState {
     double rho_old, norm_b, alpha, beta, R, omega;
     double tol, min_omega, d_omega;
     int it, maxiter, done, status;
+    int stop_le;  // 1: stop when R <= tol (cupyx cg, plain CG); 0: R < tol (MultiGrid)
 };
 
 struct Level {
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_check(const double* partial
         if (!isfinite(R)) {
             st->done = 1;
             st->status = PF_NONFINITE;
-        } else if (R < st->tol) {
+        } else if (st->stop_le ? R <= st->tol : R < st->tol) {
             st->done = 1;
             st->status = PF_OK;
         } else if (st->it >= st->maxiter) {
@@ -624,7 +625,8 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
 // ---------------------------------------------------------------------------------------
 // V-cycle (public) and PCG
 // ---------------------------------------------------------------------------------------
-__global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_omega, double d_omega, double omega) {
+__global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_omega, double d_omega, double omega,
+                             int stop_le) {
     pdl_wait();
     pdl_trigger();
     PcgState h;
@@ -635,13 +637,15 @@ __global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_o
     h.d_omega = d_omega;
     h.omega = omega;
     h.status = PF_NOT_CONVERGED;
+    h.stop_le = stop_le;
     *st = h;
 }
 
 static int init_state(pf_mg* mg, double tol, int maxiter, double omega, cudaStream_t st) {
     const double min_omega = fmax(mg->cfg.omega / 2.0, mg->cfg.min_omega);
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, mg->st, tol, maxiter, min_omega, mg->cfg.omega - min_omega, omega));
+    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, mg->st, tol, maxiter, min_omega, mg->cfg.omega - min_omega, omega,
+                       0));
     PF_LAUNCH_CHECK("state init");
     return PF_OK;
 }
@@ -903,7 +907,8 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
     PcgState* S = (PcgState*)(partials + npart);
     const int* skip = &S->done;
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, S, tol, maxiter, 0.0, 0.0, 0.0));
+    // cupyx cg (the reference CG solver, solvers/CUDA/_solvers.py:114-127) stops at ||r|| <= tol ||b||
+    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, S, tol, maxiter, 0.0, 0.0, 0.0, 1));
     if (use_x0) {
         Epi<double> e = make_epi<double>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, r, nullptr, 1.0, nullptr);
         int s = launch_fine_matvec<double, double>(op, E, x, node_mask, e, st);

@@ -114,6 +114,38 @@ def test_warm_start_and_cg():
     assert it1 < scg.last_info["iterations"]
 
 
+@pytest.mark.parametrize("case", [("cant", (8, 4, 4), 1e-9), ("mbb", (32, 16), 1e-8), ("bridge", (12, 6, 4), 1e-10)])
+def test_cg_matches_oracle_cg(case):
+    """pf_cg_solve (the CG solver) against the oracle's textbook CG, which is pinned to the
+    reference CG loop's iterates: same iteration count to within one (rounding of the
+    reductions differs), same solution, and the cupyx stopping rule ||r|| <= tol ||b||."""
+    kind, nel, tol = case
+    wl = (workloads.cantilever3d(*nel) if kind == "cant" else workloads.bridge3d(*nel) if kind == "bridge"
+          else workloads.mbb2d(*nel))
+    _, kern, sol, fe = setup_problem(wl, 1, tol=tol, maxiter=20000, solver="cg")
+    U, res = fe.solve(torch.as_tensor(wl["E"], device="cuda"))
+    xo, ito, reso = O.cg_solve(nel, unit_K0(len(nel)), wl["E"], wl["fixed_dofs"], wl["rhs"], tol=tol, maxiter=20000)
+    assert sol.last_info["status"] == "PF_OK" and sol.last_info["residual"] <= tol
+    assert abs(sol.last_info["iterations"] - ito) <= 1
+    assert rel(U.cpu().numpy(), xo) < 1e-6
+    assert true_res(kern, U, fe.rhs) < 2 * tol
+
+
+def test_cg_fixed_iterates_match_reference(golden):
+    """With tol = 0 the CG solver runs exactly maxiter iterations: its N-th iterate equals the
+    reference CG loop's (golden cg.npz, from x0 = 0)."""
+    g = golden("cg")
+    for tag, kind in (("3d", "cant"), ("2d", "mbb")):
+        nel = tuple(int(v) for v in g[tag + "_nel"])
+        wl = workloads.cantilever3d(*nel, seed=3) if kind == "cant" else workloads.mbb2d(*nel)
+        for n in g[tag + "_its"]:
+            _, kern, sol, fe = setup_problem(wl, 1, tol=0.0, maxiter=int(n), solver="cg")
+            fe.rhs.copy_(torch.as_tensor(g[tag + "_rhs"], device="cuda"))
+            U, _ = fe.solve(torch.as_tensor(g[tag + "_E"], device="cuda"))
+            assert sol.last_info["iterations"] == int(n)
+            assert rel(U.cpu().numpy(), g[f"{tag}_x{int(n)}"]) < 1e-9
+
+
 def test_status_not_converged():
     wl = workloads.cantilever3d(16, 8, 8)
     _, kern, sol, fe = setup_problem(wl, 2, tol=1e-12, maxiter=3)
