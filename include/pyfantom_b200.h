@@ -72,6 +72,10 @@ int pf_matvec_f64(const pf_op* op, const double* E, const double* u, const uint8
                   double* y, void* stream);
 int pf_matvec_f32(const pf_op* op, const float* E, const float* u, const uint8_t* node_mask,
                   float* y, void* stream);
+/* FP32 matvec with the element scales stored as BF16 (bit patterns, round-to-nearest of the
+ * FP64 E): the V-cycle operator of the mixed form with BF16 density storage. */
+int pf_matvec_f32_bf16(const pf_op* op, const uint16_t* E_bf16, const float* u, const uint8_t* node_mask,
+                       float* y, void* stream);
 /* diag(K(E)), 1 at constrained DOFs.  Replaces get_diagonal_node_basis_cuda_kernel
  * (diag.cu:1-47) behind StructuredStiffnessKernel.diagonal (_FEA.py:368-420). */
 int pf_diagonal_f64(const pf_op* op, const double* E, const uint8_t* node_mask, double* d,
@@ -104,7 +108,8 @@ typedef struct pf_mg_config {
     double min_omega;   /* reference min_omega argument (effective = max(omega/2, min_omega)) */
     double omega_boost; /* omega growth per level (reference uses 1.06) */
     double coarse_beta; /* diagonal shift of the coarse Cholesky (CHOLMOD beta = 1e-6) */
-    int precision;      /* 0 = FP64 V-cycle, 1 = FP32 V-cycle inside FP64 CG */
+    int precision;      /* 0 = FP64 V-cycle, 1 = FP32 V-cycle inside FP64 CG,
+                           2 = FP32 V-cycle reading BF16 element scales, inside FP64 CG */
     int check_every;    /* host convergence poll interval in iterations (>= 1) */
 } pf_mg_config;
 

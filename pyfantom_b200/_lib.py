@@ -69,6 +69,7 @@ SIGNATURES = {
     "pf_pack_mask": (_I, [_P, _P, _P, _P]),
     "pf_matvec_f64": (_I, [_P, _P, _P, _P, _P, _P]),
     "pf_matvec_f32": (_I, [_P, _P, _P, _P, _P, _P]),
+    "pf_matvec_f32_bf16": (_I, [_P, _P, _P, _P, _P, _P]),
     "pf_diagonal_f64": (_I, [_P, _P, _P, _P, _P]),
     "pf_sensitivity_f64": (_I, [_P, _P, _P, _P]),
     "pf_restrict_f64": (_I, [ctypes.POINTER(pf_grid), _P, _P, _P]),

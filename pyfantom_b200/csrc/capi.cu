@@ -1,3 +1,4 @@
+#include <cuda_bf16.h>
 // C ABI: library info, errors, element operator objects and single-kernel entry points.
 #include <atomic>
 #include <cstdarg>
@@ -168,6 +169,19 @@ extern "C" int pf_matvec_f32(const pf_op* op, const float* E, const float* u, co
     e.out = y;
     e.omega_scale = 1.0;
     return launch_fine_matvec<float, float>(op, E, u, node_mask, e, as_stream(stream));
+}
+
+extern "C" int pf_matvec_f32_bf16(const pf_op* op, const uint16_t* E_bf16, const float* u, const uint8_t* node_mask,
+                                  float* y, void* stream) {
+    if (!op || !E_bf16 || !u || !y) return fail(PF_BAD_ARG, "pf_matvec_f32_bf16: NULL argument");
+    if (u == y) return fail(PF_BAD_ARG, "pf_matvec_f32_bf16: u and y must not alias");
+    Epi<float> e;
+    memset(&e, 0, sizeof(e));
+    e.mode = PF_EPI_STORE;
+    e.out = y;
+    e.omega_scale = 1.0;
+    return launch_fine_matvec<float, __nv_bfloat16>(op, reinterpret_cast<const __nv_bfloat16*>(E_bf16), u, node_mask,
+                                                    e, as_stream(stream));
 }
 
 extern "C" int pf_diagonal_f64(const pf_op* op, const double* E, const uint8_t* node_mask, double* d, void* stream) {

@@ -14,8 +14,11 @@
 // either side of it along x, z neighbours are exchanged by shuffles and rows through one
 // shared-memory exchange per step.  Owner-computes: each node is written once, no atomics,
 // fixed summation order.
+#include <cuda_bf16.h>
+
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -151,6 +154,15 @@ struct H8Coef {
 // two to alternate register sets, or prefetching two planes ahead, measured slower: more
 // registers, fewer resident warps.)
 constexpr int kZTileR = 30;
+
+// element scale in the operator precision (E stored in FP64, FP32 or BF16)
+template <typename T, typename TE>
+__device__ __forceinline__ T elem_scale(TE e) {
+    if constexpr (std::is_same<TE, __nv_bfloat16>::value)
+        return (T)__bfloat162float(e);
+    else
+        return (T)e;
+}
 
 // Element operator in the Walsh basis.  glo / ghi: transformed lower / upper faces (yz
 // stages done); e: the element's scale.  Returns in G the lower-face outputs plus the
@@ -376,7 +388,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             g[c][1][1] = dn - d;
         }
     };
-    auto escale = [&](int ie) -> T { return (elem_ok && ie >= 0 && ie < NX) ? (T)E[e0 + eplane * ie] : T(0); };
+    auto escale = [&](int ie) -> T { return (elem_ok && ie >= 0 && ie < NX) ? elem_scale<T>(E[e0 + eplane * ie]) : T(0); };
 
     // One step (element ie = ix0 - 1 + s).
     //   v, m0, m1: plane ie+1 (loaded one step earlier); refilled with plane ie+2
@@ -544,7 +556,7 @@ __global__ void __launch_bounds__(256) k_matvec_q4(int NX, int NY, const T* __re
         for (int r = 0; r < 4; r++) {
             const int ei = i - kCXd(r), ej = j - kCYd(r);
             if (ei < 0 || ej < 0 || ei >= NX || ej >= NY) continue;
-            const T we = (T)E[(long long)ei * NY + ej];
+            const T we = elem_scale<T>(E[(long long)ei * NY + ej]);
             T a0 = T(0), a1 = T(0);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -666,6 +678,8 @@ template int launch_fine_matvec<double, double>(const Op*, const double*, const 
                                                 const Epi<double>&, cudaStream_t);
 template int launch_fine_matvec<float, float>(const Op*, const float*, const float*, const uint8_t*,
                                               const Epi<float>&, cudaStream_t);
+template int launch_fine_matvec<float, __nv_bfloat16>(const Op*, const __nv_bfloat16*, const float*, const uint8_t*,
+                                                      const Epi<float>&, cudaStream_t);
 
 // ---------------------------------------------------------------------------------------
 // diagonal, sensitivity, mask packing

@@ -15,6 +15,8 @@
 // iterations while the next chunk is already queued, and every kernel of an iteration
 // past convergence returns immediately.  Jacobi sweeps, residuals, the final x += e and
 // the r.z product are fused into the epilogues of the matvec kernels.
+#include <cuda_bf16.h>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -63,7 +65,8 @@ struct pf_mg {
     uint8_t* node_flag = nullptr;
     const double* E = nullptr;
     const uint8_t* mask = nullptr;
-    float* Ef = nullptr;
+    float* Ef = nullptr;            // FP32 element scales of the V-cycle (precision 1)
+    __nv_bfloat16* Eb = nullptr;    // BF16 element scales of the V-cycle (precision 2)
     double *r = nullptr, *p = nullptr, *q = nullptr;
     double* partials = nullptr;
     long long npartials = 0;
@@ -299,7 +302,8 @@ template <typename T>
 static double fine_mv_bytes(const pf_mg* mg, const T* u, const Epi<T>& e) {
     const Grid& g = mg->op->grid;
     const double D = (double)g.n_nodes * g.dof, tb = sizeof(T);
-    double b = 2.0 * D * tb + (double)g.n_elem * tb + (mg->mask ? (double)g.n_nodes : 0.0);
+    const double te = sizeof(T) == 8 ? 8.0 : (mg->Eb ? 2.0 : 4.0);  // bytes per element scale
+    double b = 2.0 * D * tb + (double)g.n_elem * te + (mg->mask ? (double)g.n_nodes : 0.0);
     if (e.mode == PF_EPI_RESID) b += D * tb;
     if (e.mode == PF_EPI_JACOBI) b += 2.0 * D * tb;
     if (e.mode == PF_EPI_JACOBI_ADD) b += 3.0 * D * tb;
@@ -314,6 +318,8 @@ static int fine_mv(pf_mg* mg, const T* u, const Epi<T>& epi, cudaStream_t st) {
     int s;
     if constexpr (sizeof(T) == 8)
         s = launch_fine_matvec<double, double>(mg->op, mg->E, u, mg->mask, epi, st);
+    else if (mg->Eb)
+        s = launch_fine_matvec<float, __nv_bfloat16>(mg->op, mg->Eb, u, mg->mask, epi, st);
     else
         s = launch_fine_matvec<float, float>(mg->op, mg->Ef, u, mg->mask, epi, st);
     if (s) return s;
@@ -432,6 +438,7 @@ static void mg_free(pf_mg* mg) {
     }
     dense_free(&mg->dense);
     for (void* p : {(void*)mg->K0_dev, (void*)mg->Kc_dev, (void*)mg->elem_flag, (void*)mg->node_flag, (void*)mg->Ef,
+                    (void*)mg->Eb,
                     (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st,
                     (void*)mg->Eint, (void*)mg->bi, (void*)mg->xi})
         if (p) cudaFree(p);
@@ -462,7 +469,8 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     *out = nullptr;
     if (cfg->n_level < 1 || cfg->n_level > kMaxLevel) return fail(PF_BAD_ARG, "n_level must be in [1, %d]", kMaxLevel);
     if (cfg->n_smooth < 1 || cfg->n_smooth > 64) return fail(PF_BAD_ARG, "n_smooth must be in [1, 64]");
-    if (cfg->precision != 0 && cfg->precision != 1) return fail(PF_BAD_ARG, "precision must be 0 (fp64) or 1 (fp32)");
+    if (cfg->precision < 0 || cfg->precision > 2)
+        return fail(PF_BAD_ARG, "precision must be 0 (fp64), 1 (fp32 V-cycle) or 2 (fp32 V-cycle, bf16 densities)");
     const Grid& g = op->grid;
     for (int a = 0; a < g.dim; a++)
         if (g.nel[a] % (1 << cfg->n_level) != 0)
@@ -471,7 +479,7 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     mg->op = op;
     mg->cfg = *cfg;
     if (mg->cfg.check_every < 1) mg->cfg.check_every = 1;
-    mg->fp32 = cfg->precision;
+    mg->fp32 = cfg->precision != 0 ? 1 : 0;
     mg->nlev = cfg->n_level;
     const size_t ts = mg->fp32 ? sizeof(float) : sizeof(double);
     int s = PF_OK;
@@ -507,7 +515,8 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     s = s ? s : dalloc((void**)&mg->elem_flag, (size_t)g1.n_elem);
     s = s ? s : dalloc((void**)&mg->node_flag, (size_t)g1.n_nodes);
     const long long n0 = mg->L[0].ndof;
-    if (mg->fp32) s = s ? s : dalloc((void**)&mg->Ef, (size_t)g.n_elem * sizeof(float));
+    if (cfg->precision == 1) s = s ? s : dalloc((void**)&mg->Ef, (size_t)g.n_elem * sizeof(float));
+    if (cfg->precision == 2) s = s ? s : dalloc((void**)&mg->Eb, (size_t)g.n_elem * sizeof(__nv_bfloat16));
     s = s ? s : dalloc((void**)&mg->r, n0 * sizeof(double));
     s = s ? s : dalloc((void**)&mg->p, n0 * sizeof(double));
     s = s ? s : dalloc((void**)&mg->q, n0 * sizeof(double));
@@ -582,7 +591,11 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
         if ((s = launch_diagonal<float>(mg->op, E, node_mask, (float*)L0.dinv, st))) return s;
         pf::count_launch();
         k_recip<float><<<vec_blocks(L0.ndof), kRedThreads, 0, st>>>(L0.ndof, (float*)L0.dinv);
-        if ((s = launch_d2f(g.n_elem, E, mg->Ef, st))) return s;
+        if (mg->Eb) {
+            if ((s = launch_d2bf(g.n_elem, E, mg->Eb, st))) return s;
+        } else if ((s = launch_d2f(g.n_elem, E, mg->Ef, st))) {
+            return s;
+        }
     } else {
         if ((s = launch_diagonal<double>(mg->op, E, node_mask, (double*)L0.dinv, st))) return s;
         pf::count_launch();

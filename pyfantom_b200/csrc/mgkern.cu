@@ -699,4 +699,18 @@ int launch_d2f(long long n, const double* a, float* b, cudaStream_t st) {
     return PF_OK;
 }
 
+__global__ void k_d2bf(long long n, const double* __restrict__ a, __nv_bfloat16* __restrict__ b) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = __double2bfloat16(a[i]);
+}
+int launch_d2bf(long long n, const double* a, __nv_bfloat16* b, cudaStream_t st) {
+    long long nb = (n + 255) / 256;
+    if (nb > 4 * kNumSM * 8) nb = 4 * kNumSM * 8;
+    if (nb < 1) nb = 1;
+    pf::count_launch();
+    k_d2bf<<<(unsigned)nb, 256, 0, st>>>(n, a, b);
+    PF_LAUNCH_CHECK("d2bf launch");
+    return PF_OK;
+}
+
 }  // namespace pf

@@ -1,6 +1,8 @@
 // Launchers of the multigrid level kernels (mgkern.cu) and the dense coarse solver (dense.cu).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace pf {
@@ -38,6 +40,8 @@ template <typename T>
 int launch_stencil_dinv(const Grid& g, const double* A, T* dinv, cudaStream_t st);
 int launch_stencil_to_dense(const Grid& g, const double* A, double* M, long long ld, cudaStream_t st);
 int launch_d2f(long long n, const double* a, float* b, cudaStream_t st);
+// FP64 -> BF16 (round to nearest even)
+int launch_d2bf(long long n, const double* a, __nv_bfloat16* b, cudaStream_t st);
 
 // dense SPD coarse solver: factor (M + beta I) of order n (padded to a multiple of 32,
 // ld = padded order) and form its inverse; x = inv * b.

@@ -8,8 +8,9 @@
   reference's V-cycle, damped-Jacobi smoother, adaptive omega schedule, Galerkin
   hierarchy and normalised transfers; the coarse solve is a dense Cholesky on the
   device instead of host CHOLMOD (every reference ``coarse_solver`` name maps to it,
-  with the same ``beta = 1e-6`` shift).  Keyword-only extras: ``precision`` ('fp64' or
-  'mixed': FP32 V-cycle inside the FP64 CG), ``check_every`` (host poll interval) and
+  with the same ``beta = 1e-6`` shift).  Keyword-only extras: ``precision`` ('fp64',
+  'mixed': FP32 V-cycle inside the FP64 CG, or 'mixed_bf16': the same with the V-cycle's
+  fine-level element scales stored as BF16), ``check_every`` (host poll interval) and
   ``warm_start`` (an object with ``guess(kernel, rhs)``, e.g. learned.LearnedWarmStart,
   that supplies the initial guess of a solve that does not reuse ``last_x0``).
 
@@ -176,8 +177,8 @@ class MultiGrid(Solver):
             # the reference only takes its W branch for a lower-case 'w'; the default 'W'
             # runs V-cycles, which is what this solver implements
             raise NotImplementedError("the lower-case 'w' (W-cycle) branch is not implemented; use 'V' or 'W'")
-        if precision not in ("fp64", "mixed"):
-            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if precision not in ("fp64", "mixed", "mixed_bf16"):
+            raise ValueError("precision must be 'fp64', 'mixed' or 'mixed_bf16'")
         self._min_omega_arg = min_omega
         self._mg = None
         self.last_info = None
@@ -192,7 +193,7 @@ class MultiGrid(Solver):
         cfg.min_omega = float(self._min_omega_arg)
         cfg.omega_boost = float(self.omega_boost)
         cfg.coarse_beta = 1e-6
-        cfg.precision = 0 if self.precision == "fp64" else 1
+        cfg.precision = {"fp64": 0, "mixed": 1, "mixed_bf16": 2}[self.precision]
         cfg.check_every = int(self.check_every)
         h = ctypes.c_void_p()
         _lib.check(_lib.load().pf_mg_create(self.kernel._op, ctypes.byref(cfg), ctypes.byref(h)))

@@ -357,3 +357,29 @@ def test_dot(lib):
     at, bt = T(a), T(b)
     lib.check(L.pf_dot_f64(a.size, lib.ptr(at), lib.ptr(bt), lib.ptr(res), lib.ptr(work), lib.stream()))
     assert abs(N(res)[0] - a @ b) < 1e-10 * np.abs(a * b).sum()
+
+
+def _bf16_round(E):
+    """E rounded to BF16 (round to nearest even), back as float64."""
+    return torch.as_tensor(E, dtype=torch.float64).to(torch.bfloat16).to(torch.float64).numpy()
+
+
+@pytest.mark.parametrize("nel", [(16, 8, 8), (40, 9, 33), (7, 5, 95), (65, 33)])
+def test_matvec_bf16_element_scales(lib, nel):
+    """FP32 matvec reading BF16 element scales: equal to the oracle's matvec with E rounded to
+    BF16 (the only approximation is the storage of E) to FP32 rounding, 2e-5; the BF16
+    rounding itself moves the product by at most 2^-8 relative to the FP64-E one."""
+    rng = np.random.default_rng(sum(nel) + 3)
+    op = Op(lib, nel)
+    E = rng.uniform(1e-3, 1.0, int(np.prod(nel)))
+    u = rng.standard_normal(op.ndof).astype(np.float32)
+    cons = rng.choice(op.ndof, size=max(1, op.ndof // 9), replace=False)
+    L = lib
+    Eb = torch.as_tensor(E, device="cuda").to(torch.bfloat16)
+    ut = T(u, torch.float32)
+    y = torch.full_like(ut, float("nan"))
+    m = op.mask(cons)
+    L.check(L.load().pf_matvec_f32_bf16(op.h, L.ptr(Eb), L.ptr(ut), L.ptr(m), L.ptr(y), L.stream()))
+    got = N(y)
+    assert rel(got, O.matvec(nel, op.K0, _bf16_round(E), u.astype(np.float64), cons)) < 2e-5
+    assert rel(got, O.matvec(nel, op.K0, E, u.astype(np.float64), cons)) < 2 ** -8

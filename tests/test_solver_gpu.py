@@ -84,13 +84,14 @@ def test_mgcg_matches_reference_solution(golden):
     assert rel(U.cpu().numpy(), g["mg_U"]) < 1e-8
 
 
-@pytest.mark.parametrize("nel", [(32, 16, 16), (64, 32)])
-def test_mixed_precision_reaches_fp64_tolerance(nel):
+@pytest.mark.parametrize("nel,prec", [((32, 16, 16), "mixed"), ((64, 32), "mixed"), ((32, 16, 16), "mixed_bf16"),
+                                      ((64, 32), "mixed_bf16")])
+def test_mixed_precision_reaches_fp64_tolerance(nel, prec):
     wl = workloads.cantilever3d(*nel) if len(nel) == 3 else workloads.mbb2d(*nel)
     E = torch.as_tensor(wl["E"], device="cuda")
     _, k64, s64, fe64 = setup_problem(wl, 3, "fp64", tol=1e-8)
     U64, _ = fe64.solve(E)
-    _, k32, s32, fe32 = setup_problem(wl, 3, "mixed", tol=1e-8)
+    _, k32, s32, fe32 = setup_problem(wl, 3, prec, tol=1e-8)
     U32, res = fe32.solve(E)
     assert s32.last_info["status"] == "PF_OK"
     assert true_res(k32, U32, fe32.rhs) < 2e-8
@@ -260,3 +261,26 @@ def test_full_size_cantilever_matches_reference(precision):
         assert true_res(kern, U, fe.rhs) < 1.5e-8
         c = float(torch.dot(fe.rhs, U))
         assert abs(c - 7.472352867980982) < 1e-6 * 7.472352867980982
+
+
+@pytest.mark.parametrize("prec", ["mixed_bf16", "mixed"])
+def test_simp_loop_mixed_forms_track_fp64(prec):
+    """The 192x96x96 configuration's loop at 64x32x32: SIMP + OC with the displacement solves
+    in the mixed form (FP32 V-cycle, BF16 or FP32 element scales), every iteration's
+    stiffness also solved by the FP64 MGCG at the same tolerance: relative compliance error
+    below 1e-6 and displacement error below 1e-5 at every iteration."""
+    from pyfantom_b200.CUDA import MinimumCompliance, MultiGrid, OC, StructuredFilter3D
+    wl = workloads.cantilever3d(64, 32, 32)
+    mesh, kern, sol, fe = setup_problem(wl, 4, prec, tol=1e-8, maxiter=1000)
+    ref = MultiGrid(mesh, kern, maxiter=1000, tol=1e-8, n_smooth=2, omega=0.6, n_level=4, precision="fp64")
+    prob = MinimumCompliance(fe, StructuredFilter3D(mesh, 2.0), E_mul=[1.0], void=1e-9, penalty=3.0,
+                             volume_fraction=[0.3], heavyside=False)
+    oc = OC(prob, move=0.2)
+    for it in range(6):
+        if it:
+            oc.iter()
+        assert sol.last_info["status"] == "PF_OK"
+        Ur, _ = ref.solve(fe.rhs, use_last=True)
+        cr = float(torch.dot(fe.rhs, Ur))
+        assert abs(float(prob.f()) - cr) < 1e-6 * abs(cr)
+        assert float(torch.linalg.norm(prob._U - Ur) / torch.linalg.norm(Ur)) < 1e-5
