@@ -139,6 +139,9 @@ int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, i
  * device milliseconds, launches, and algorithmic bytes (each operand counted once). */
 int pf_mg_set_profiling(pf_mg* mg, int max_launches);
 int pf_mg_profile(const pf_mg* mg, double* h_ms, long long* h_launches, double* h_bytes);
+/* Which fine-level matvec launches the profiling records: 1 = the FP64 ones (PCG matvec,
+ * FP64 V-cycle), 2 = the FP32 ones (V-cycle of the mixed forms), 3 = both (default). */
+int pf_mg_profile_select(pf_mg* mg, int which);
 /* Number of doubles of device workspace pf_cg_solve needs for `op`. */
 size_t pf_cg_workspace_size(const pf_op* op);
 /* Unpreconditioned CG on K(E) x = b (the matrix-free CG of _solvers.py:22-132).  `work`
@@ -244,6 +247,14 @@ int pf_cnn_guess_f64(const pf_grid* fine, int P, const float* coarse_nodes, cons
  * doubles; work[size - 2] = alpha, work[size - 1] = ||b - alpha Kx0|| / ||b||. */
 size_t pf_cnn_energy_scale_workspace(void);
 int pf_cnn_energy_scale_f64(long long n, double* x0, const double* Kx0, const double* b, double* work, void* stream);
+/* Of two initial guesses xa, xb of K u = f (with Kxa, Kxb their products), write to out the
+ * one whose energy-optimal multiple alpha x (alpha = x.f / x.Kx) has the lower energy
+ * -(x.f)^2 / (2 x.Kx), i.e. the smaller energy-norm error; a guess with x.Kx <= 0 counts as
+ * the zero start.  out may alias xa or xb.  work: pf_cnn_guess_select_workspace() doubles;
+ * its last four hold {alpha, choice (0 = xa, 1 = xb), energy of xa, energy of xb}. */
+size_t pf_cnn_guess_select_workspace(void);
+int pf_cnn_guess_select_f64(long long n, const double* xa, const double* Kxa, const double* xb, const double* Kxb,
+                            const double* f, double* out, double* work, void* stream);
 
 /* Energy-deficit training loss of a nodal prediction y for K u = b (y zero on constrained
  * DOFs, Ky = K y, c = b.u > 0): loss = 1 - (b.y)^2 / ((y.Ky) c), the relative energy

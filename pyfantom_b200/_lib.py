@@ -62,6 +62,7 @@ SIGNATURES = {
     "pf_launch_count": (ctypes.c_ulonglong, []),
     "pf_mg_set_profiling": (_I, [_P, _I]),
     "pf_mg_profile": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_LL), ctypes.POINTER(_D)]),
+    "pf_mg_profile_select": (_I, [_P, _I]),
     "pf_last_error": (ctypes.c_char_p, []),
     "pf_status_string": (ctypes.c_char_p, [_I]),
     "pf_op_create": (_I, [ctypes.POINTER(pf_grid), _P, ctypes.POINTER(_P)]),
@@ -126,6 +127,8 @@ SIGNATURES = {
     "pf_cnn_guess_f64": (_I, [ctypes.POINTER(pf_grid), _I, _P, _P, _P, _P]),
     "pf_cnn_energy_scale_workspace": (_SZ, []),
     "pf_cnn_energy_scale_f64": (_I, [_LL, _P, _P, _P, _P, _P]),
+    "pf_cnn_guess_select_workspace": (_SZ, []),
+    "pf_cnn_guess_select_f64": (_I, [_LL, _P, _P, _P, _P, _P, _P, _P, _P]),
     "pf_cnn_energy_loss_workspace": (_SZ, []),
     "pf_cnn_energy_loss_f64": (_I, [_LL, _P, _P, _P, _D, _P, _P, _P, _P]),
 }

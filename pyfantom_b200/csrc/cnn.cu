@@ -742,6 +742,67 @@ extern "C" int pf_cnn_energy_scale_f64(long long n, double* x0, const double* Kx
     return PF_OK;
 }
 
+// Choice between two initial guesses a, b of K u = f: each scaled by its energy-optimal
+// factor alpha = (x.f) / (x.Kx), the one with the lower energy -(x.f)^2 / (2 x.Kx) (the
+// smaller energy-norm error) is written to out (a guess with x.Kx <= 0 counts as the zero
+// start).  stats = {alpha, choice (0 = a, 1 = b), energy of a, energy of b}.
+__global__ void __launch_bounds__(256) k_select_partials(long long n, const double* __restrict__ xa,
+                                                         const double* __restrict__ ka, const double* __restrict__ xb,
+                                                         const double* __restrict__ kb, const double* __restrict__ f,
+                                                         double* __restrict__ part) {
+    __shared__ double red[8];
+    double s[4] = {0.0, 0.0, 0.0, 0.0};  // xa.f, xa.Kxa, xb.f, xb.Kxb
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double fi = f[i], a = xa[i], b = xb[i];
+        s[0] += a * fi;
+        s[1] += a * ka[i];
+        s[2] += b * fi;
+        s[3] += b * kb[i];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const double t = block_sum<256>(s[q], red);
+        if (threadIdx.x == 0) part[q * kScaleBlocks + blockIdx.x] = t;
+    }
+}
+__global__ void k_select_apply(long long n, const double* __restrict__ part, const double* xa, const double* xb,
+                               double* out, double* __restrict__ stats) {
+    double s[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        s[q] = 0.0;
+        for (int i = 0; i < kScaleBlocks; i++) s[q] += part[q * kScaleBlocks + i];
+    }
+    const double ea = s[1] > 0.0 ? -0.5 * s[0] * s[0] / s[1] : 0.0;
+    const double eb = s[3] > 0.0 ? -0.5 * s[2] * s[2] / s[3] : 0.0;
+    const bool pick_b = eb < ea;
+    const double alpha = pick_b ? (s[3] > 0.0 ? s[2] / s[3] : 0.0) : (s[1] > 0.0 ? s[0] / s[1] : 0.0);
+    const double* x = pick_b ? xb : xa;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        stats[0] = alpha;
+        stats[1] = pick_b ? 1.0 : 0.0;
+        stats[2] = ea;
+        stats[3] = eb;
+    }
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = alpha * x[i];
+}
+
+extern "C" size_t pf_cnn_guess_select_workspace(void) { return 4 * kScaleBlocks + 4; }
+
+extern "C" int pf_cnn_guess_select_f64(long long n, const double* xa, const double* Kxa, const double* xb,
+                                       const double* Kxb, const double* f, double* out, double* work, void* stream) {
+    if (n < 1 || !xa || !Kxa || !xb || !Kxb || !f || !out || !work)
+        return fail(PF_BAD_ARG, "pf_cnn_guess_select_f64: bad argument");
+    if (out == Kxa || out == Kxb || out == f) return fail(PF_BAD_ARG, "pf_cnn_guess_select_f64: out aliases an input");
+    cudaStream_t st = as_stream(stream);
+    count_launch(2);
+    k_select_partials<<<kScaleBlocks, 256, 0, st>>>(n, xa, Kxa, xb, Kxb, f, work);
+    k_select_apply<<<gs(n), 256, 0, st>>>(n, work, xa, xb, out, work + 4 * kScaleBlocks);
+    PF_LAUNCH_CHECK("guess select launch");
+    return PF_OK;
+}
+
 extern "C" size_t pf_cnn_energy_loss_workspace(void) { return 2 * kScaleBlocks; }
 
 extern "C" int pf_cnn_energy_loss_f64(long long n, const double* y, const double* Ky, const double* b, double c,

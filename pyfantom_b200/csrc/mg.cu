@@ -87,6 +87,7 @@ struct pf_mg {
     unsigned long long g_start_nodes[2] = {0, 0}, g_chunk_nodes = 0;
     const uint8_t* g_mask = nullptr;  // node mask the graphs were captured with
     int profile = 0;
+    int profile_which = 3;         // bit 0: FP64 fine matvec launches, bit 1: FP32 ones
     std::vector<cudaEvent_t> pev;  // pairs (start, end)
     std::vector<double> pbytes;    // algorithmic bytes of each recorded launch
     int pn = 0;
@@ -313,7 +314,8 @@ static double fine_mv_bytes(const pf_mg* mg, const T* u, const Epi<T>& e) {
 
 template <typename T>
 static int fine_mv(pf_mg* mg, const T* u, const Epi<T>& epi, cudaStream_t st) {
-    const bool rec = mg->profile && mg->pn < (int)mg->pev.size() / 2;
+    const bool rec = mg->profile && mg->pn < (int)mg->pev.size() / 2 &&
+                     (mg->profile_which & (sizeof(T) == 8 ? 1 : 2)) != 0;
     if (rec) PF_CUDA(cudaEventRecord(mg->pev[2 * mg->pn], st));
     int s;
     if constexpr (sizeof(T) == 8)
@@ -1009,6 +1011,12 @@ extern "C" int pf_mg_set_profiling(pf_mg* mg, int max_launches) {
         mg->pev.push_back(e);
     }
     mg->pbytes.assign(max_launches, 0.0);
+    return PF_OK;
+}
+
+extern "C" int pf_mg_profile_select(pf_mg* mg, int which) {
+    if (!mg || which < 1 || which > 3) return fail(PF_BAD_ARG, "pf_mg_profile_select: which must be 1, 2 or 3");
+    mg->profile_which = which;
     return PF_OK;
 }
 

@@ -485,14 +485,18 @@ class LearnedWarmStart:
     """Initial guess of the MGCG from the network (see the module docstring).
 
     ``pool`` = P sets the network's cell grid to nel / P (each count divisible by 8 P).
+    ``with_previous``: in a sequence of solves (the SIMP loop, where the solver reuses the
+    last solution), offer both the network's guess and the previous solution and start
+    from the one with the lower energy (``guess(..., prev=...)``).
     After every guess, ``last`` holds {alpha, residual}: the energy-optimal scale and the
     relative residual ||b - K x0|| / ||b|| of the scaled guess (read back only when
     ``read_stats``)."""
 
-    def __init__(self, net: WarmStartNet, pool: int = 1, read_stats: bool = True):
+    def __init__(self, net: WarmStartNet, pool: int = 1, read_stats: bool = True, with_previous: bool = False):
         self.net = net
         self.pool = int(pool)
         self.read_stats = read_stats
+        self.with_previous = bool(with_previous)
         self.last = None
         self.x0 = None
         self._scratch = {}
@@ -506,13 +510,18 @@ class LearnedWarmStart:
             cells = (1, N_IN, nel[0] // P, nel[1] // P, nel[2] // P)
             self._scratch = {key: dict(
                 x0=torch.empty(n, dtype=torch.float64, device=dev), kx=torch.empty(n, dtype=torch.float64, device=dev),
+                kp=torch.empty(n, dtype=torch.float64, device=dev), xs=torch.empty(n, dtype=torch.float64, device=dev),
+                sel=torch.empty(int(_lib.load().pf_cnn_guess_select_workspace()), dtype=torch.float64, device=dev),
                 feat=torch.empty(cells, dtype=torch.float32, device=dev),
                 work=torch.zeros(1, dtype=torch.int32, device=dev),
                 scale=torch.empty(int(_lib.load().pf_cnn_energy_scale_workspace()), dtype=torch.float64, device=dev))}
         return self._scratch[key]
 
-    def guess(self, kern, rhs):
-        """Scaled initial guess for K(rho) u = rhs with the kernel's current rho."""
+    def guess(self, kern, rhs, prev=None):
+        """Scaled initial guess for K(rho) u = rhs with the kernel's current rho.  With
+        ``prev`` (the previous solution of a sequence of solves, e.g. the last SIMP
+        iteration's displacements) the guess is whichever of the network's prediction and
+        ``prev``, each energy-optimally scaled, has the lower energy."""
         L = _lib.load()
         n = rhs.shape[0]
         b = self._buf(n, kern)
@@ -523,6 +532,18 @@ class LearnedWarmStart:
         _lib.check(L.pf_cnn_guess_f64(ctypes.byref(g), self.pool, _p(nodes), kern._mask_ptr(), _p(b["x0"]),
                                       _lib.stream()))
         _lib.check(L.pf_matvec_f64(kern._op, _p(kern.rho), _p(b["x0"]), kern._mask_ptr(), _p(b["kx"]), _lib.stream()))
+        if prev is not None:
+            prev = as_cuda(prev, torch.float64)
+            _lib.check(L.pf_matvec_f64(kern._op, _p(kern.rho), _p(prev), kern._mask_ptr(), _p(b["kp"]),
+                                       _lib.stream()))
+            _lib.check(L.pf_cnn_guess_select_f64(n, _p(b["x0"]), _p(b["kx"]), _p(prev), _p(b["kp"]), _p(rhs),
+                                                 _p(b["xs"]), _p(b["sel"]), _lib.stream()))
+            self.x0 = b["xs"]
+            if self.read_stats:
+                a, which, ea, eb = b["sel"][-4:].tolist()
+                self.last = dict(alpha=a, choice="previous" if which else "network", energy_network=ea,
+                                 energy_previous=eb)
+            return b["xs"]
         _lib.check(L.pf_cnn_energy_scale_f64(n, _p(b["x0"]), _p(b["kx"]), _p(rhs), _p(b["scale"]), _lib.stream()))
         self.x0 = b["x0"]
         if self.read_stats:

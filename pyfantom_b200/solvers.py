@@ -234,7 +234,9 @@ class MultiGrid(Solver):
         rhs = as_cuda(rhs, torch.float64)
         n = rhs.shape[0]
         warm = use_last and self.last_x0 is not None
-        if warm:
+        if warm and self.warm_start is not None and getattr(self.warm_start, "with_previous", False):
+            x = self.warm_start.guess(k, rhs, prev=self.last_x0).clone()
+        elif warm:
             x = self.last_x0
         elif self.warm_start is not None:
             x = self.warm_start.guess(k, rhs).clone()

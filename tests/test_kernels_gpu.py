@@ -383,3 +383,32 @@ def test_matvec_bf16_element_scales(lib, nel):
     got = N(y)
     assert rel(got, O.matvec(nel, op.K0, _bf16_round(E), u.astype(np.float64), cons)) < 2e-5
     assert rel(got, O.matvec(nel, op.K0, E, u.astype(np.float64), cons)) < 2 ** -8
+
+
+def test_guess_select_picks_lower_energy(lib):
+    """pf_cnn_guess_select_f64 on a small SPD system: the chosen guess is the energy-optimal
+    multiple of the candidate with the lower energy -(x.f)^2 / (2 x.Kx)."""
+    L = lib.load()
+    rng = np.random.default_rng(5)
+    n = 3000
+    d = rng.uniform(1.0, 2.0, n)
+    f = rng.standard_normal(n)
+    u = f / d  # exact solution of the diagonal system K = diag(d)
+    for xa, xb in [(u + 0.1 * rng.standard_normal(n), rng.standard_normal(n)),
+                   (rng.standard_normal(n), 2.0 * u + 0.01 * rng.standard_normal(n)),
+                   (np.zeros(n), u)]:
+        ta, tb, tf = T(xa), T(xb), T(f)
+        ka, kb = T(d * xa), T(d * xb)
+        out = torch.empty_like(ta)
+        work = torch.empty(int(L.pf_cnn_guess_select_workspace()), dtype=torch.float64, device="cuda")
+        lib.check(L.pf_cnn_guess_select_f64(n, lib.ptr(ta), lib.ptr(ka), lib.ptr(tb), lib.ptr(kb), lib.ptr(tf),
+                                            lib.ptr(out), lib.ptr(work), lib.stream()))
+
+        def energy(x):
+            q = x @ (d * x)
+            return -0.5 * (x @ f) ** 2 / q if q > 0 else 0.0
+        best = xb if energy(xb) < energy(xa) else xa
+        q = best @ (d * best)
+        want = (best @ f) / q * best if q > 0 else np.zeros(n)
+        assert rel(N(out), want) < 1e-12
+        assert N(work)[-3] == (1.0 if best is xb else 0.0)
