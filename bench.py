@@ -1,28 +1,38 @@
 #!/usr/bin/env python
 """Benchmark: MGCG solves/s of the structured SIMP elasticity solve, one JSON line.
 
-Workload (default ``cantilever_96x48x48``): 96x48x48 H8 cantilever, 698,691 DOF, E0=1,
-Emin=1e-9, nu=0.3, penal=3, densities seeded uniform(0.001,1) Gaussian-smoothed (sigma=2);
-plain FP64 MultiGrid-preconditioned CG, 4 coarse levels, 2 pre/post damped-Jacobi sweeps
-(omega=0.6, reference adaptive schedule), relative residual 1e-8, cold start (x0 = 0).
-One step = one complete solve including the hierarchy setup (the densities change every
-SIMP iteration, so the hierarchy is rebuilt every solve, as in the reference).
+Headline workload (default ``cantilever_256x128x128``): 256x128x128 H8 cantilever,
+12,830,211 DOF, E0=1, Emin=1e-9, nu=0.3, penal=3, densities seeded uniform(0.001,1)
+Gaussian-smoothed (sigma=2); MultiGrid-preconditioned CG with 5 coarse levels, 2 pre/post
+damped-Jacobi sweeps (omega=0.6, reference adaptive schedule), relative residual 1e-8.
+The timed form (default ``mixed_learned``) is the mixed-precision solver (FP32 V-cycle
+inside the FP64 CG) started from the learned initial guess (network on the 64x32x32 pooled
+cell grid; its inference is inside the timed solve).  One step = one complete solve
+including the hierarchy setup (the densities change every SIMP iteration, so the hierarchy
+is rebuilt every solve, as in the reference).  The plain FP64 MGCG and the other forms are
+timed beside it (``forms``), with their compliance and displacement errors against FP64,
+and the SIMP loops of the 192x96x96 (BF16 densities, 20 iterations) and 256x128x128
+(learned guess, 30 iterations) configurations report per-iteration errors against FP64.
 
 Arms
   default          this library on N GPUs (one process per GPU, replicas: a solve does not
                    shard; ranks run independent solves, ``scaling: weak``).
   --impl reference the reference algorithm on the host CPU: the C/OpenMP restatement of the
-                   reference MultiGrid solve (all host threads), same workload and metric.
+                   reference MultiGrid solve (FP64, all host threads), same workload and
+                   metric, timed on a bounded sample (hierarchy setup + K PCG iterations,
+                   extrapolated to the iteration count of the complete solve).
 
 Timing: W untimed warm-up solves, then K solves, each bracketed by CUDA events on the
-solve stream with a 512 MB L2 flush before each; max over ranks.  ``e2e`` repeats the
-measurement through the public API with the loads and densities in pinned host memory
-(host->device copies and the device->host copy of U inside the timed region).
+solve stream with a 512 MB L2 flush before each (the inputs exceed L2 as well); max over
+ranks.  ``e2e`` repeats the measurement through the public API (FiniteElement.solve) with
+the loads and densities in pinned host memory (host->device copies and the device->host
+copy of U inside the timed region).
 """
 from __future__ import annotations
 
 import argparse
 import csv
+import ctypes
 import io
 import json
 import os
@@ -42,7 +52,11 @@ WORKLOADS = {
     "cantilever_192x96x96": dict(nel=(192, 96, 96), n_level=5),
     "cantilever_256x128x128": dict(nel=(256, 128, 128), n_level=5),
 }
-METRIC = "MGCG solves/sec (rel-res 1e-8)"
+# form -> (MultiGrid precision, learned initial guess)
+FORMS = {"fp64": ("fp64", False), "mixed": ("mixed", False), "mixed_bf16": ("mixed_bf16", False),
+         "mixed_learned": ("mixed", True)}
+METRIC = "MGCG solves/sec and matvec HBM GB/s, mixed+learned vs plain FP64 at rel-res 1e-8"
+KNOWN = os.path.join(ROOT, "tests", "golden", "known_answers.json")
 
 
 def peaks():
@@ -51,6 +65,15 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def full_iterations(workload):
+    """PCG iterations of the complete FP64 solve of the workload (the oracle's complete
+    solve, recorded in the known answers), or None."""
+    try:
+        return int(json.load(open(KNOWN))[workload + "_oracle"]["pcg_iterations"])
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 # -----------------------------------------------------------------------------------------
@@ -113,21 +136,40 @@ class Clocks:
 # -----------------------------------------------------------------------------------------
 # our arm
 # -----------------------------------------------------------------------------------------
-def build_problem(nel, n_level, precision="fp64", tol=1e-8, warm_start=None):
+_NET = None
+
+
+def warm_start_for(learned, with_previous=False):
+    global _NET
+    if not learned:
+        return None
+    from pyfantom_b200 import learned as L
+    if _NET is None:
+        _NET = L.WarmStartNet.load()
+    return L.LearnedWarmStart(_NET, pool=4, read_stats=False, with_previous=with_previous)
+
+
+def build_problem(nel, n_level, form="fp64", tol=1e-8, with_previous=False):
     import torch
     from pyfantom_b200 import workloads
     from pyfantom_b200.CUDA import FiniteElement, MultiGrid, StructuredMesh3D, StructuredStiffnessKernel
     from pyfantom_b200.physics import LinearElasticity
+    prec, learned = FORMS[form]
     wl = workloads.cantilever3d(*nel)
     mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
     kern = StructuredStiffnessKernel(mesh)
-    sol = MultiGrid(mesh, kern, maxiter=1000, tol=tol, n_smooth=2, omega=0.6, n_level=n_level, precision=precision,
-                    warm_start=warm_start)
+    sol = MultiGrid(mesh, kern, maxiter=1000, tol=tol, n_smooth=2, omega=0.6, n_level=n_level, precision=prec,
+                    warm_start=warm_start_for(learned, with_previous))
     fe = FiniteElement(mesh, kern, sol)
     fe.add_dirichlet_boundary_condition(node_ids=torch.as_tensor(wl["fixed_nodes"], device="cuda"), rhs=0.0)
     fe.add_point_forces(forces=wl["load_forces"], node_ids=torch.as_tensor(wl["load_nodes"], device="cuda"))
     E = torch.as_tensor(wl["E"], device="cuda")
     return wl, mesh, kern, sol, fe, E
+
+
+def _flush_buffer():
+    import torch
+    return torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
 
 def run_ours(args, rank, world, local_rank):
@@ -139,9 +181,9 @@ def run_ours(args, rank, world, local_rank):
     lib = _lib.load()
     spec = WORKLOADS[args.workload]
     nel, nl = spec["nel"], spec["n_level"]
-    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, args.precision)
+    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, args.form)
     D, Ne = kern.shape[0], int(np.prod(nel))
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = _flush_buffer()
     stream = torch.cuda.current_stream()
 
     def solve_once():
@@ -200,7 +242,7 @@ def run_ours(args, rank, world, local_rank):
         e0.record(stream)
         fe.rhs.copy_(rhs_h, non_blocking=True)
         E_dev.copy_(E_h, non_blocking=True)
-        fe.solver.last_x0 = None  # every timed solve starts from x0 = 0
+        fe.solver.last_x0 = None  # every timed solve starts cold (x0 = 0, or the learned guess)
         U2, _ = fe.solve(E_dev)
         U_h.copy_(U2, non_blocking=True)
         e1.record(stream)
@@ -211,38 +253,46 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_max = float(te.item())
 
-    # ---- roofline of the dominant kernel: fine FP64 matvec, timed live in one solve ----
+    # ---- roofline of the dominant kernel: the fine-level matvec of the V-cycle (FP32 in
+    # the mixed forms, FP64 in the FP64 form), every launch of one solve timed live with
+    # CUDA events on the solve's stream --------------------------------------------------
+    fp32 = FORMS[args.form][0] != "fp64"
     lib.pf_mg_set_profiling(sol._mg, 20000)
+    lib.pf_mg_profile_select(sol._mg, 2 if fp32 else 1)
     flush.fill_(1.0)
     solve_once()
-    import ctypes
     ms, n_l, byts = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
     lib.pf_mg_profile(sol._mg, ctypes.byref(ms), ctypes.byref(n_l), ctypes.byref(byts))
     lib.pf_mg_set_profiling(sol._mg, 0)
     avg_us = ms.value / max(n_l.value, 1) * 1e3
     achieved = byts.value / max(ms.value, 1e-12) / 1e6  # GB/s
     hbm, peak_kind = peaks()
+    kname = "k_matvec_h8p<float> / k_matvec_h8r<float>" if fp32 else "k_matvec_h8r<double>"
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
-            "kernel": "k_matvec_h8r<double> (fine-level stiffness matvec, register x-march, fused epilogues)",
+            "kernel": f"{kname} (fine-level stiffness matvec of the V-cycle, register x-march, fused epilogues)",
             "launches_in_solve": int(n_l.value), "avg_launch_us": round(avg_us, 2),
             "algorithmic_bytes_per_launch": round(byts.value / max(n_l.value, 1))}
     prof_path = os.path.join(ROOT, "profiles", "matvec_h8_traffic.json")
     if os.path.exists(prof_path):
-        tr = json.load(open(prof_path)).get(args.workload)
+        tr = json.load(open(prof_path)).get(f"{args.workload}/{args.form}")
         if tr:
             roof["traffic"] = tr.get("dram_bytes_per_launch")
             roof["traffic_source"] = tr.get("source")
 
+    dtype = {"fp64": "f64", "mixed": "f64 outer / f32 V-cycle", "mixed_bf16": "f64 outer / f32 V-cycle / bf16 E",
+             "mixed_learned": "f64 outer / f32 V-cycle"}[args.form]
     result = {
         "metric": METRIC, "value": round(world * args.steps / (max_ms / 1e3), 4), "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 outer / f32 V-cycle",
+        "vs_baseline": None, "dtype": dtype,
         "data": "synthetic (seeded smoothed-random densities, cantilever loads)",
-        "config": {"workload": args.workload, "nel": list(nel), "dof": D, "n_level": nl, "n_smooth": 2,
-                   "omega": 0.6, "tol": 1e-8, "precision": args.precision, "start": "cold (x0 = 0)",
-                   "l2": "512 MB L2 flush before every timed solve", "parallelism": f"replicas x{world}",
+        "config": {"workload": args.workload, "form": args.form, "nel": list(nel), "dof": D, "n_level": nl,
+                   "n_smooth": 2, "omega": 0.6, "tol": 1e-8,
+                   "start": "learned guess (network on nel/4 cells)" if FORMS[args.form][1] else "cold (x0 = 0)",
+                   "l2": "512 MB L2 flush before every timed solve; inputs exceed L2",
+                   "parallelism": f"replicas x{world}",
                    "warmup_extra": "untimed solves until 1 s has passed, so the clocks settle"},
         "pcg_iterations": iters, "status": status, "compliance": compliance,
         "e2e": {"value": round(world * args.steps / (e2e_max / 1e3), 4), "unit": "solves/s",
@@ -252,163 +302,188 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0:
         result["clocks"] = clk
-    return result, (wl, mesh)
+    del wl, mesh, kern, sol, fe, E, U, flush
+    torch.cuda.empty_cache()
+    return result
 
 
-def forms_256():
-    """The three solver forms at the 256x128x128 cantilever (12.8M DOF, 5 levels, tol 1e-8,
-    cold start): plain FP64 MGCG, mixed precision (FP32 V-cycle in FP64 CG) and mixed
-    precision from the learned guess (network on the 64x32x32 pooled cell grid, trilinear
-    interpolation, energy-optimal scale; its inference is inside the timed solve).  Each
-    form: median of 3 timed solves after 1 warm-up, L2 flushed before each."""
+def time_form(nel, nl, form, reps=3, ref=None):
+    """Median of `reps` cold solves (after one warm-up) of one form, L2 flushed before each,
+    with the true residual and (given the FP64 reference (compliance, U)) the errors."""
     import torch
-    from pyfantom_b200 import learned
-    nel, nl = (256, 128, 128), 5
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    out, ref = {}, None
-    ws = learned.LearnedWarmStart(learned.WarmStartNet.load(), pool=4, read_stats=False)
-    for name, prec, w in (("fp64", "fp64", None), ("mixed", "mixed", None), ("mixed_learned", "mixed", ws)):
-        wl, mesh, kern, sol, fe, E = build_problem(nel, nl, prec, warm_start=w)
-        kern.set_rho(E)
-        U, _ = sol.solve(fe.rhs, use_last=False)
-        t = []
-        for _ in range(3):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            kern.set_rho(E)
-            U, _ = sol.solve(fe.rhs, use_last=False)
-            e1.record()
-            e1.synchronize()
-            t.append(e0.elapsed_time(e1))
-        r = fe.rhs - kern.dot(U)
-        c = float(torch.dot(fe.rhs, U))
-        ms = statistics.median(t)
-        out[name] = {"solves_per_s": round(1e3 / ms, 3), "ms": round(ms, 2),
-                     "pcg_iterations": sol.last_info["iterations"],
-                     "true_rel_residual": float(torch.linalg.norm(r) / torch.linalg.norm(fe.rhs)),
-                     "compliance": c}
-        if ref is None:
-            ref = (c, U.clone())
-        else:
-            out[name]["rel_compliance_err_vs_fp64"] = abs(c - ref[0]) / abs(ref[0])
-            out[name]["rel_displacement_err_vs_fp64"] = float(torch.linalg.norm(U - ref[1]) / torch.linalg.norm(ref[1]))
-            out[name]["speedup_vs_fp64"] = round(out["fp64"]["ms"] / ms, 3)
-        del wl, mesh, kern, sol, fe, E, U, r
-    if ws.x0 is not None:
-        out["mixed_learned"]["guess"] = "network on 64x32x32 cells (pool 4), energy-scaled"
-    return out
-
-
-def extras(args):
-    """Secondary measurements on one GPU: mixed-precision form at the same workload, the
-    fine matvec at 256x128x128 (HBM-resident) in FP64 and FP32, and the three solver forms
-    at 256x128x128."""
-    import torch
-    out = {}
-    spec = WORKLOADS[args.workload]
-    wl, mesh, kern, sol, fe, E = build_problem(spec["nel"], spec["n_level"], "mixed")
+    flush = _flush_buffer()
+    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, form)
     kern.set_rho(E)
-    for _ in range(2):
-        U, _ = sol.solve(fe.rhs, use_last=False)
-    torch.cuda.synchronize()
+    U, _ = sol.solve(fe.rhs, use_last=False)
     t = []
-    for _ in range(3):
+    for _ in range(reps):
+        flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
+        kern.set_rho(E)
         U, _ = sol.solve(fe.rhs, use_last=False)
         e1.record()
         e1.synchronize()
         t.append(e0.elapsed_time(e1))
     r = fe.rhs - kern.dot(U)
-    out["mixed_precision"] = {"solves_per_s": round(1e3 / statistics.median(t), 3),
-                              "pcg_iterations": sol.last_info["iterations"],
-                              "true_rel_residual": float(torch.linalg.norm(r) / torch.linalg.norm(fe.rhs)),
-                              "compliance": float(torch.dot(fe.rhs, U))}
-    del wl, mesh, kern, sol, fe, E
-    # fine matvec at 256x128x128, L2 flushed between launches
-    from pyfantom_b200 import _lib
-    from pyfantom_b200 import workloads
-    from pyfantom_b200.CUDA import StructuredMesh3D, StructuredStiffnessKernel
-    from pyfantom_b200.physics import LinearElasticity
-    nel = (256, 128, 128)
-    w5 = workloads.cantilever3d(*nel)
-    mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
-    kern = StructuredStiffnessKernel(mesh)
-    kern.add_constraints(torch.as_tensor(w5["fixed_dofs"], device="cuda"))
-    D, Ne, Nn = kern.shape[0], int(np.prod(nel)), kern.n_nodes
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    lib = _lib.load()
-    for prec, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
-        Et = torch.as_tensor(w5["E"], device="cuda").to(dt)
-        u = torch.randn(D, dtype=dt, device="cuda")
-        y = torch.empty_like(u)
-        f = lib.pf_matvec_f64 if dt == torch.float64 else lib.pf_matvec_f32
-        ts = []
-        for i in range(8):
-            flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            _lib.check(f(kern._op, _lib.ptr(Et), _lib.ptr(u), _lib.ptr(kern.node_mask), _lib.ptr(y), _lib.stream()))
-            e1.record()
-            e1.synchronize()
-            if i >= 2:
-                ts.append(e0.elapsed_time(e1))
-        ms = statistics.median(ts)
-        sz = 4 if dt == torch.float32 else 8
-        byts = 2 * D * sz + Ne * sz + Nn
-        out[f"matvec_256x128x128_{prec}"] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts,
-                                             "GB_per_s": round(byts / ms / 1e6, 1),
-                                             "dof_matvecs_per_s": round(D / ms * 1e3, 1)}
-    del kern, mesh, u, y, Et
-    out["forms_256x128x128"] = forms_256()
+    c = float(torch.dot(fe.rhs, U))
+    ms = statistics.median(t)
+    out = {"solves_per_s": round(1e3 / ms, 3), "ms": round(ms, 2), "pcg_iterations": sol.last_info["iterations"],
+           "setup_ms": round(sol.last_info["setup_ms"], 2),
+           "true_rel_residual": float(torch.linalg.norm(r) / torch.linalg.norm(fe.rhs)), "compliance": c}
+    if ref is not None:
+        out["rel_compliance_err_vs_fp64"] = abs(c - ref[0]) / abs(ref[0])
+        out["rel_displacement_err_vs_fp64"] = float(torch.linalg.norm(U - ref[1]) / torch.linalg.norm(ref[1]))
+    keep = (c, U.clone())
+    del wl, mesh, kern, sol, fe, E, U, r, flush
+    torch.cuda.empty_cache()
+    return out, keep
+
+
+def forms_at(workload, names=("fp64", "mixed", "mixed_bf16", "mixed_learned")):
+    """The solver forms at one workload; speed-ups and errors against the plain FP64 MGCG."""
+    spec = WORKLOADS[workload]
+    out, ref = {}, None
+    for name in names:
+        o, keep = time_form(spec["nel"], spec["n_level"], name, ref=ref)
+        if ref is None:
+            ref = keep
+        else:
+            o["speedup_vs_fp64"] = round(out["fp64"]["ms"] / o["ms"], 3)
+        out[name] = o
+    if "mixed_learned" in out:
+        out["mixed_learned"]["guess"] = "network on nel/4 cells, energy-scaled"
     return out
 
 
-def probe_matvec(args):
-    """Time the fine-level matvec alone (FP64 and FP32, L2 flushed before every launch)."""
+def matvec_probe(workload, reps=8, warm=2):
+    """The fine matvec alone (FP64, FP32, FP32 with BF16 element scales), L2 flushed before
+    every launch: microseconds, algorithmic bytes and GB/s, DOF-matvecs/s."""
     import torch
     from pyfantom_b200 import _lib, workloads
     from pyfantom_b200.CUDA import StructuredMesh3D, StructuredStiffnessKernel
     from pyfantom_b200.physics import LinearElasticity
-    nel = WORKLOADS[args.workload]["nel"]
+    nel = WORKLOADS[workload]["nel"]
     w = workloads.cantilever3d(*nel)
     mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
     kern = StructuredStiffnessKernel(mesh)
     kern.add_constraints(torch.as_tensor(w["fixed_dofs"], device="cuda"))
     D, Ne, Nn = kern.shape[0], int(np.prod(nel)), kern.n_nodes
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = _flush_buffer()
     lib = _lib.load()
-    out = {"probe": "matvec", "workload": args.workload}
-    for prec, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
-        Et = torch.as_tensor(w["E"], device="cuda").to(dt)
+    hbm, kind = peaks()
+    out = {}
+    E64 = torch.as_tensor(w["E"], device="cuda")
+    for prec in ("fp64", "fp32", "fp32_bf16E"):
+        dt = torch.float64 if prec == "fp64" else torch.float32
+        if prec == "fp32_bf16E":
+            Et, esz = E64.to(torch.bfloat16), 2
+            f = lib.pf_matvec_f32_bf16
+        else:
+            Et, esz = E64.to(dt), (8 if prec == "fp64" else 4)
+            f = lib.pf_matvec_f64 if prec == "fp64" else lib.pf_matvec_f32
         u = torch.randn(D, dtype=dt, device="cuda")
         y = torch.empty_like(u)
-        f = lib.pf_matvec_f64 if dt == torch.float64 else lib.pf_matvec_f32
         ts = []
-        for i in range(args.warmup + args.steps):
+        for i in range(warm + reps):
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             _lib.check(f(kern._op, _lib.ptr(Et), _lib.ptr(u), _lib.ptr(kern.node_mask), _lib.ptr(y), _lib.stream()))
             e1.record()
             e1.synchronize()
-            if i >= args.warmup:
+            if i >= warm:
                 ts.append(e0.elapsed_time(e1))
         ms = statistics.median(ts)
-        sz = 4 if dt == torch.float32 else 8
-        byts = 2 * D * sz + Ne * sz + Nn
-        out[prec] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts, "GB_per_s": round(byts / ms / 1e6, 1)}
+        sz = 8 if prec == "fp64" else 4
+        byts = 2 * D * sz + Ne * esz + Nn
+        out[prec] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts, "GB_per_s": round(byts / ms / 1e6, 1),
+                     "frac_of_hbm": round(byts / ms / 1e6 / hbm, 4), "dof_matvecs_per_s": round(D / ms * 1e3, 1)}
+    out["peak"] = {"GB_per_s": hbm, "kind": kind}
+    del kern, mesh, u, y, Et, flush
+    torch.cuda.empty_cache()
     return out
 
 
+def simp_loop(workload, form, n_iter, vf=0.3, r_min=2.0, move=0.2):
+    """SIMP minimum compliance with OC on the workload, the displacement solves by `form`
+    (the learned form offers the network's guess and the previous solution, whichever has
+    the lower energy).  Each iteration's stiffness is also solved by the plain FP64 MGCG
+    (warm-started from its own previous solution, same tolerance) to give the relative
+    compliance and displacement errors of the form; the time per SIMP iteration (filter,
+    penalisation, solve, sensitivity, adjoint filter, OC update) excludes those checks."""
+    import torch
+    from pyfantom_b200.CUDA import MinimumCompliance, MultiGrid, OC, StructuredFilter3D
+    spec = WORKLOADS[workload]
+    nel, nl = spec["nel"], spec["n_level"]
+    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, form, with_previous=True)
+    ref = MultiGrid(mesh, kern, maxiter=1000, tol=1e-8, n_smooth=2, omega=0.6, n_level=nl, precision="fp64")
+    prob = MinimumCompliance(fe, StructuredFilter3D(mesh, r_min), E_mul=[1.0], void=1e-9, penalty=3.0,
+                             volume_fraction=[vf], heavyside=False)
+    oc = OC(prob, move=move)
+    x0 = torch.as_tensor(wl["x"], device="cuda")
+    prob.set_desvars(x0)
+    oc.last_desvars = x0.clone()
+    oc.last_f = prob.f()
+    rows, t_iter, its = [], [], []
+
+    def check(row):
+        U = prob._U
+        Ur, _ = ref.solve(fe.rhs, use_last=True)
+        cr = float(torch.dot(fe.rhs, Ur))
+        c = float(prob.f())
+        row.update(compliance=c, rel_compliance_err=abs(c - cr) / abs(cr),
+                   rel_displacement_err=float(torch.linalg.norm(U - Ur) / torch.linalg.norm(Ur)),
+                   pcg_iterations=sol.last_info["iterations"], fp64_pcg_iterations=ref.last_info["iterations"])
+        rows.append(row)
+
+    check({"iteration": 0})
+    for it in range(n_iter):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        oc.iter()
+        e1.record()
+        e1.synchronize()
+        t_iter.append(e0.elapsed_time(e1))
+        its.append(sol.last_info["iterations"])
+        check({"iteration": it + 1, "ms": round(t_iter[-1], 2)})
+    out = {"workload": workload, "form": form, "iterations": n_iter, "volfrac": vf, "r_min": r_min,
+           "ms_per_simp_iteration": round(statistics.mean(t_iter), 2),
+           "mean_pcg_iterations": round(statistics.mean(its), 2),
+           "max_rel_compliance_err": max(r["rel_compliance_err"] for r in rows),
+           "max_rel_displacement_err": max(r["rel_displacement_err"] for r in rows),
+           "per_iteration": [{k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in r.items()}
+                             for r in rows]}
+    del wl, mesh, kern, sol, fe, E, ref, prob, oc
+    torch.cuda.empty_cache()
+    return out
+
+
+def extras(args):
+    """Secondary measurements on one GPU: the forms at the workload, the fine matvec alone,
+    the forms at 192x96x96, and the two SIMP loops."""
+    out = {"forms": forms_at(args.workload), "matvec": matvec_probe(args.workload)}
+    if args.workload != "cantilever_192x96x96":
+        out["forms_192x96x96"] = forms_at("cantilever_192x96x96", ("fp64", "mixed", "mixed_bf16"))
+    if not args.no_simp:
+        out["simp_192x96x96_mixed_bf16"] = simp_loop("cantilever_192x96x96", "mixed_bf16", 20)
+        out["simp_256x128x128_mixed_learned"] = simp_loop("cantilever_256x128x128", "mixed_learned", 30)
+    return out
+
+
+def probe_matvec(args):
+    """Time the fine-level matvec alone (for ncu captures)."""
+    return {"probe": "matvec", "workload": args.workload, **matvec_probe(args.workload, reps=args.steps,
+                                                                           warm=args.warmup)}
+
+
 def probe_solve(args):
-    """One cold solve of the workload after two warm-up solves, bracketed by
+    """One solve of the workload after two warm-up solves, bracketed by
     cudaProfilerStart/Stop (for `ncu --profile-from-start off`: the launch list of exactly
     one solve, hierarchy setup included)."""
     import torch
     spec = WORKLOADS[args.workload]
-    wl, mesh, kern, sol, fe, E = build_problem(spec["nel"], spec["n_level"], args.precision)
+    wl, mesh, kern, sol, fe, E = build_problem(spec["nel"], spec["n_level"], args.form)
     kern.set_rho(E)
     for _ in range(2):
         sol.solve(fe.rhs, use_last=False)
@@ -417,7 +492,7 @@ def probe_solve(args):
     U, res = sol.solve(fe.rhs, use_last=False)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
-    return {"probe": "solve", "workload": args.workload, "precision": args.precision,
+    return {"probe": "solve", "workload": args.workload, "form": args.form,
             "iterations": sol.last_info["iterations"], "status": sol.last_info["status"],
             "solve_ms": sol.last_info["solve_ms"], "setup_ms": sol.last_info["setup_ms"]}
 
@@ -425,39 +500,50 @@ def probe_solve(args):
 # -----------------------------------------------------------------------------------------
 # reference arm and CPU baseline: the oracle (C/OpenMP restatement of the reference solve)
 # -----------------------------------------------------------------------------------------
-def cpu_solve(nel, n_level):
+def cpu_sample(workload, k_iters):
+    """The oracle's FP64 MGCG on the workload: hierarchy setup plus k PCG iterations, timed
+    separately; the complete solve's time is extrapolated to its iteration count."""
     from oracle import oracle as O
     from pyfantom_b200 import workloads
-    from pyfantom_b200.physics import LinearElasticity
     from pyfantom_b200.geom import _unit_element
-    wl = workloads.cantilever3d(*nel)
+    from pyfantom_b200.physics import LinearElasticity
+    spec = WORKLOADS[workload]
+    wl = workloads.cantilever3d(*spec["nel"])
     K0 = LinearElasticity(E=1.0, nu=0.3).K(_unit_element((1.0, 1.0, 1.0)))
-    t = time.perf_counter()
-    x, it, res, st = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=n_level, n_smooth=2,
-                                  omega=0.6, tol=1e-8)
-    return time.perf_counter() - t, it, float(wl["rhs"] @ x), O.num_threads()
+    x, it, res, st, setup_s, iter_s = O.mgcg_solve_timed(spec["nel"], K0, wl["E"], wl["fixed_dofs"], wl["rhs"],
+                                                         n_level=spec["n_level"], n_smooth=2, omega=0.6, tol=1e-8,
+                                                         maxiter=k_iters)
+    n_full = full_iterations(workload)
+    complete = st == 0  # converged inside the sample: a complete solve
+    if complete or n_full is None:
+        n_full = it
+    solve_s = setup_s + iter_s / max(it, 1) * n_full
+    return dict(solve_s=solve_s, setup_s=setup_s, iter_s_each=iter_s / max(it, 1), iters_sampled=it,
+                iters_full=n_full, complete=complete, threads=O.num_threads(),
+                compliance=float(wl["rhs"] @ x) if complete else None)
 
 
 def run_reference(args):
     spec = WORKLOADS[args.workload]
-    warm = min(args.warmup, 1)  # compiled C: one untimed solve warms caches and page tables
-    for _ in range(warm):
-        cpu_solve(spec["nel"], spec["n_level"])
-    ts = []
-    for _ in range(args.steps):
-        dt, it, c, threads = cpu_solve(spec["nel"], spec["n_level"])
-        ts.append(dt)
-    total = sum(ts)
-    v = args.steps / total
+    # one sample: the setup and K PCG iterations (compiled C needs no warm-up); the complete
+    # solve's time is extrapolated from it
+    s = cpu_sample(args.workload, args.steps)
+    v = 1.0 / s["solve_s"]
+    sample = (f"hierarchy setup + {s['iters_sampled']} PCG iterations of the FP64 MGCG solve "
+              f"({s['setup_s']:.2f} s + {s['iter_s_each']:.3f} s per iteration), extrapolated to the "
+              f"{s['iters_full']} iterations of the complete solve")
+    if s["complete"]:
+        sample = f"one complete solve ({s['iters_full']} PCG iterations)"
     return {
-        "metric": METRIC, "value": round(v, 5), "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
-        "warmup": warm, "ms_per_step": round(total / args.steps * 1e3, 1), "higher_is_better": True,
+        "metric": METRIC, "value": round(v, 6), "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": 0, "ms_per_step": round(s["solve_s"] * 1e3, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": args.workload, "nel": list(spec["nel"]), "n_level": spec["n_level"], "tol": 1e-8},
-        "pcg_iterations": it, "compliance": c,
-        "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} complete solves of the workload on the host CPU"},
-        "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": args.workload, "form": "fp64", "nel": list(spec["nel"]), "n_level": spec["n_level"],
+                   "n_smooth": 2, "omega": 0.6, "tol": 1e-8, "start": "cold (x0 = 0)"},
+        "pcg_iterations": s["iters_full"],
+        "cpu_baseline": {"value": round(v, 6), "unit": "solves/s", "cores": s["threads"], "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(v, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
@@ -467,14 +553,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cantilever_96x48x48", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="cantilever_256x128x128", choices=sorted(WORKLOADS))
+    ap.add_argument("--form", default="mixed_learned", choices=sorted(FORMS))
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-simp", action="store_true", help="skip the SIMP loops in the extras")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=3, help="PCG iterations of the CPU-baseline sample")
     ap.add_argument("--probe", choices=["matvec", "solve"], default=None,
-                    help="only time the fine matvec (FP64 and FP32) at the workload size (for ncu captures)")
+                    help="only time the fine matvec or bracket one solve (for ncu captures)")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" and not args.probe else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -497,16 +585,22 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    result, _ = run_ours(args, rank, world, local_rank)
+    result = run_ours(args, rank, world, local_rank)
     if rank == 0 and world == 1 and not args.no_extras:
-        result["forms"] = extras(args)
+        ex = extras(args)
+        result["forms"] = ex
+        f = ex["forms"]
+        if "fp64" in f and args.form in f:
+            result["fp64_solves_per_s"] = f["fp64"]["solves_per_s"]
+            result["speedup_vs_fp64"] = round(f["fp64"]["ms"] / f[args.form]["ms"], 3)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        spec = WORKLOADS[args.workload]
-        if spec["nel"] == (96, 48, 48):
-            dt, it, c, threads = cpu_solve(spec["nel"], spec["n_level"])
-            result["cpu_baseline"] = {"value": round(1.0 / dt, 5), "unit": "solves/s", "cores": threads, "kind": "port",
-                                      "sample": "one complete solve of the workload (C/OpenMP oracle, all host threads)",
-                                      "pcg_iterations": it, "compliance": c}
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        s = cpu_sample(args.workload, args.cpu_iters)
+        result["cpu_baseline"] = {
+            "value": round(1.0 / s["solve_s"], 6), "unit": "solves/s", "cores": s["threads"], "kind": "port",
+            "sample": (f"C/OpenMP oracle FP64 MGCG: hierarchy setup + {s['iters_sampled']} PCG iterations "
+                       f"({s['setup_s']:.2f} s + {s['iter_s_each']:.3f} s per iteration), extrapolated to the "
+                       f"{s['iters_full']} iterations of the complete solve")}
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
