@@ -111,6 +111,9 @@ typedef struct pf_mg_config {
     int precision;      /* 0 = FP64 V-cycle, 1 = FP32 V-cycle inside FP64 CG,
                            2 = FP32 V-cycle reading BF16 element scales, inside FP64 CG */
     int check_every;    /* host convergence poll interval in iterations (>= 1) */
+    int coarse_op;      /* 0 = level 1 applied element by element from the fine densities when
+                           K0 is an isotropic box element and level 1 is smoothed (else its
+                           stencil); 1 = assembled stencils on every level */
 } pf_mg_config;
 
 typedef struct pf_solve_info {
@@ -134,6 +137,13 @@ int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega, void* stre
  * Blocks the calling thread until the solve ends; info is filled on return. */
 int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, int maxiter,
                 pf_solve_info* info, void* stream);
+/* y = A_l u with the operator the V-cycle applies on level l in [0, n_level) (l = 0: the
+ * fine matvec; l = 1: the element-level operator or the stencil; deeper: the stencil), in
+ * the V-cycle precision (double for precision 0, float otherwise).  Requires pf_mg_setup. */
+int pf_mg_level_matvec(pf_mg* mg, int level, const void* u, void* y, void* stream);
+/* h_elem_level1 = 1 if level 1 is applied element by element; h_dirty = its number of
+ * coarse elements with an explicit matrix (those touching a constraint). */
+int pf_mg_level_info(const pf_mg* mg, int* h_elem_level1, int* h_dirty);
 /* Diagnostics: time every fine-level matvec launch of the following solves with CUDA
  * events (at most max_launches per solve; 0 disables), and read the last solve's totals:
  * device milliseconds, launches, and algorithmic bytes (each operand counted once). */

@@ -37,7 +37,7 @@ class pf_grid(ctypes.Structure):
 class pf_mg_config(ctypes.Structure):
     _fields_ = [("n_level", ctypes.c_int), ("n_smooth", ctypes.c_int), ("omega", ctypes.c_double),
                 ("min_omega", ctypes.c_double), ("omega_boost", ctypes.c_double), ("coarse_beta", ctypes.c_double),
-                ("precision", ctypes.c_int), ("check_every", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("check_every", ctypes.c_int), ("coarse_op", ctypes.c_int)]
 
 
 class pf_solve_info(ctypes.Structure):
@@ -63,6 +63,8 @@ SIGNATURES = {
     "pf_mg_set_profiling": (_I, [_P, _I]),
     "pf_mg_profile": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_LL), ctypes.POINTER(_D)]),
     "pf_mg_profile_select": (_I, [_P, _I]),
+    "pf_mg_level_matvec": (_I, [_P, _I, _P, _P, _P]),
+    "pf_mg_level_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "pf_last_error": (ctypes.c_char_p, []),
     "pf_status_string": (ctypes.c_char_p, [_I]),
     "pf_op_create": (_I, [ctypes.POINTER(pf_grid), _P, ctypes.POINTER(_P)]),

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 
+#include "coarse.cuh"
 #include "common.cuh"
 #include "elemop.cuh"
 #include "mgkern.cuh"
@@ -65,6 +66,7 @@ struct pf_mg {
     uint8_t* node_flag = nullptr;
     const double* E = nullptr;
     const uint8_t* mask = nullptr;
+    pf::CoarseOp* c1 = nullptr;     // element-level operator of level 1 (else its stencil)
     float* Ef = nullptr;            // FP32 element scales of the V-cycle (precision 1)
     __nv_bfloat16* Eb = nullptr;    // BF16 element scales of the V-cycle (precision 2)
     double *r = nullptr, *p = nullptr, *q = nullptr;
@@ -336,6 +338,7 @@ static int fine_mv(pf_mg* mg, const T* u, const Epi<T>& epi, cudaStream_t st) {
 template <typename T>
 static int level_matvec(pf_mg* mg, int l, const T* u, const Epi<T>& epi, cudaStream_t st) {
     if (l == 0) return fine_mv<T>(mg, u, epi, st);
+    if (l == 1 && mg->c1) return launch_coarse_matvec<T>(mg->c1, mg->L[1].g, u, epi, st);
     return launch_stencil_matvec<T>(mg->L[l].g, (const T*)mg->L[l].H, u, epi, st, true);
 }
 
@@ -439,6 +442,8 @@ static void mg_free(pf_mg* mg) {
         L = Level();
     }
     dense_free(&mg->dense);
+    coarse_destroy(mg->c1);
+    mg->c1 = nullptr;
     for (void* p : {(void*)mg->K0_dev, (void*)mg->Kc_dev, (void*)mg->elem_flag, (void*)mg->node_flag, (void*)mg->Ef,
                     (void*)mg->Eb,
                     (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st,
@@ -485,6 +490,16 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     mg->nlev = cfg->n_level;
     const size_t ts = mg->fp32 ? sizeof(float) : sizeof(double);
     int s = PF_OK;
+    if (cfg->coarse_op != 0 && cfg->coarse_op != 1) {
+        delete mg;
+        return fail(PF_BAD_ARG, "coarse_op must be 0 (element operator on level 1 when available) or 1 (stencils)");
+    }
+    // level 1 element by element when it is smoothed (not the coarsest) and K0 allows it
+    if (cfg->coarse_op == 0 && g.dim == 3 && mg->nlev >= 2) {
+        double coef[150];
+        if (coarse_factorise(op, coef) == PF_OK) s = coarse_create(op, mg->fp32, &mg->c1);
+        if (!s) set_error("");
+    }
     Grid gl = g;
     for (int l = 0; l <= mg->nlev && !s; l++) {
         Level& L = mg->L[l];
@@ -502,7 +517,7 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
         if (l >= 1) {
             const size_t nst = (size_t)gl.n_nodes * (gl.dim == 3 ? 27 : 9) * gl.dof * gl.dof;
             s = s ? s : dalloc((void**)&L.A64, nst * sizeof(double));
-            if (l < mg->nlev) s = s ? s : dalloc(&L.H, (size_t)stencil_half_size(gl) * ts);
+            if (l < mg->nlev && !(l == 1 && mg->c1)) s = s ? s : dalloc(&L.H, (size_t)stencil_half_size(gl) * ts);
         }
         gl = coarse_grid(gl);
     }
@@ -618,13 +633,22 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
         if ((s = launch_galerkin_l1p(mg->L[l - 1].g, mg->L[l - 1].A64, mg->L[l].A64, st))) return s;
     for (int l = 1; l < mg->nlev; l++) {
         Level& L = mg->L[l];
-        const long long nst = L.g.n_nodes * (L.g.dim == 3 ? 27 : 9) * L.g.dof * L.g.dof;
+        const bool half = L.H != nullptr;  // level 1 with the element operator has no stencil copy
         if (mg->fp32) {
             if ((s = launch_stencil_dinv<float>(L.g, L.A64, (float*)L.dinv, st))) return s;
-            if ((s = launch_stencil_half<float>(L.g, L.A64, (float*)L.H, st))) return s;
+            if (half && (s = launch_stencil_half<float>(L.g, L.A64, (float*)L.H, st))) return s;
         } else {
             if ((s = launch_stencil_dinv<double>(L.g, L.A64, (double*)L.dinv, st))) return s;
-            if ((s = launch_stencil_half<double>(L.g, L.A64, (double*)L.H, st))) return s;
+            if (half && (s = launch_stencil_half<double>(L.g, L.A64, (double*)L.H, st))) return s;
+        }
+    }
+    if (mg->c1) {
+        bool moved = false;
+        if ((s = coarse_setup(mg->c1, E, node_mask, mg->elem_flag, mg->K0_dev, st, &moved))) return s;
+        if (moved) {  // the captured graphs hold the old dirty storage: recapture
+            for (cudaGraphExec_t& gx : mg->g_start)
+                if (gx) cudaGraphExecDestroy(gx), gx = nullptr;
+            if (mg->g_chunk) cudaGraphExecDestroy(mg->g_chunk), mg->g_chunk = nullptr;
         }
     }
     // coarsest: dense factor and inverse
@@ -997,6 +1021,28 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
 // ---------------------------------------------------------------------------------------
 // profiling of the fine-level matvec inside a solve
 // ---------------------------------------------------------------------------------------
+extern "C" int pf_mg_level_matvec(pf_mg* mg, int level, const void* u, void* y, void* stream) {
+    if (!mg || !u || !y) return fail(PF_BAD_ARG, "pf_mg_level_matvec: NULL argument");
+    if (!mg->ready) return fail(PF_BAD_ARG, "pf_mg_level_matvec: call pf_mg_setup first");
+    if (level < 0 || level >= mg->nlev)
+        return fail(PF_BAD_ARG, "pf_mg_level_matvec: level must be in [0, %d)", mg->nlev);
+    if (u == y) return fail(PF_BAD_ARG, "pf_mg_level_matvec: u and y must not alias");
+    cudaStream_t st = as_stream(stream);
+    if (mg->fp32) {
+        Epi<float> e = make_epi<float>(PF_EPI_STORE, nullptr, nullptr, nullptr, nullptr, (float*)y, nullptr, 1.0, nullptr);
+        return level_matvec<float>(mg, level, (const float*)u, e, st);
+    }
+    Epi<double> e = make_epi<double>(PF_EPI_STORE, nullptr, nullptr, nullptr, nullptr, (double*)y, nullptr, 1.0, nullptr);
+    return level_matvec<double>(mg, level, (const double*)u, e, st);
+}
+
+extern "C" int pf_mg_level_info(const pf_mg* mg, int* h_elem_level1, int* h_dirty) {
+    if (!mg || !h_elem_level1 || !h_dirty) return fail(PF_BAD_ARG, "pf_mg_level_info: NULL argument");
+    *h_elem_level1 = mg->c1 ? 1 : 0;
+    *h_dirty = mg->c1 ? mg->c1->ndirty : 0;
+    return PF_OK;
+}
+
 extern "C" int pf_mg_set_profiling(pf_mg* mg, int max_launches) {
     if (!mg || max_launches < 0) return fail(PF_BAD_ARG, "pf_mg_set_profiling: bad argument");
     PF_CUDA(cudaDeviceSynchronize());

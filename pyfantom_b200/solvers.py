@@ -12,7 +12,9 @@
   'mixed': FP32 V-cycle inside the FP64 CG, or 'mixed_bf16': the same with the V-cycle's
   fine-level element scales stored as BF16), ``check_every`` (host poll interval) and
   ``warm_start`` (an object with ``guess(kernel, rhs)``, e.g. learned.LearnedWarmStart,
-  that supplies the initial guess of a solve that does not reuse ``last_x0``).
+  that supplies the initial guess of a solve that does not reuse ``last_x0``) and
+  ``coarse_op`` ('element': level 1 applied element by element from the fine densities
+  when the element allows it, the default; 'stencil': assembled stencils on every level).
 
 ``solve(rhs, rho=None, use_last=True)`` returns ``(U, residual)`` like the reference;
 ``last_x0`` holds the warm start.  Solver statistics of the last call are in
@@ -144,7 +146,7 @@ class MultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="cholmod", matrix_free=False, low_level_tol=1e-8,
                  low_level_maxiter=5000, min_omega=0.4, omega_boost=1.06, *, precision="fp64", check_every=4,
-                 warm_start=None):
+                 warm_start=None, coarse_op="element"):
         self.kernel = kernel
         self.warm_start = warm_start
         self.mesh = mesh
@@ -179,6 +181,9 @@ class MultiGrid(Solver):
             raise NotImplementedError("the lower-case 'w' (W-cycle) branch is not implemented; use 'V' or 'W'")
         if precision not in ("fp64", "mixed", "mixed_bf16"):
             raise ValueError("precision must be 'fp64', 'mixed' or 'mixed_bf16'")
+        if coarse_op not in ("element", "stencil"):
+            raise ValueError("coarse_op must be 'element' or 'stencil'")
+        self.coarse_op = coarse_op
         self._min_omega_arg = min_omega
         self._mg = None
         self.last_info = None
@@ -195,6 +200,7 @@ class MultiGrid(Solver):
         cfg.coarse_beta = 1e-6
         cfg.precision = {"fp64": 0, "mixed": 1, "mixed_bf16": 2}[self.precision]
         cfg.check_every = int(self.check_every)
+        cfg.coarse_op = 0 if self.coarse_op == "element" else 1
         h = ctypes.c_void_p()
         _lib.check(_lib.load().pf_mg_create(self.kernel._op, ctypes.byref(cfg), ctypes.byref(h)))
         self._mg = h
@@ -224,6 +230,22 @@ class MultiGrid(Solver):
         w = self.min_omega if omega is None else float(omega)
         _lib.check(_lib.load().pf_mg_vcycle(self._mg, _lib.ptr(r), _lib.ptr(z), w, _lib.stream()))
         return z
+
+    def level_matvec(self, level, u):
+        """y = A_level u with the operator the V-cycle applies on that level (needs setup());
+        float64 for precision 'fp64', float32 otherwise."""
+        dt = torch.float64 if self.precision == "fp64" else torch.float32
+        u = as_cuda(u, dt)
+        y = torch.empty_like(u)
+        _lib.check(_lib.load().pf_mg_level_matvec(self._mg, int(level), _lib.ptr(u), _lib.ptr(y), _lib.stream()))
+        return y
+
+    def level_info(self):
+        """(level 1 applied element by element, number of its coarse elements with an
+        explicit matrix) of the current hierarchy."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.load().pf_mg_level_info(self._mg, ctypes.byref(a), ctypes.byref(b)))
+        return bool(a.value), int(b.value)
 
     def solve(self, rhs, rho=None, use_last=True):
         k = self.kernel
