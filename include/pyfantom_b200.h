@@ -217,6 +217,20 @@ int pf_cnn_conv3d_fwd_f32(const float* x, int N, int Cin, int X, int Y, int Z, c
 /* dx = W^T dy (accumulate != 0: dx += W^T dy) */
 int pf_cnn_conv3d_bwd_data_f32(const float* dy, int N, int Cin, int X, int Y, int Z, const float* w, int Cout,
                                int stride, int accumulate, float* dx, void* stream);
+/* The forward and the input gradient on the tensor cores (tcgen05.mma implicit GEMM): same
+ * arguments and layouts as the FP32 versions, operands rounded to BF16, accumulation in
+ * FP32; at most 256 output channels.  err (device int, set to 0 by the caller) becomes 1 if
+ * a wait for the tensor cores ran out (the output is then not written). */
+int pf_cnn_conv3d_fwd_tc(const float* x, int N, int Cin, int X, int Y, int Z, const float* w, const float* b,
+                         int Cout, int stride, int relu, float* y, int* err, void* stream);
+int pf_cnn_conv3d_bwd_data_tc(const float* dy, int N, int Cin, int X, int Y, int Z, const float* w, int Cout,
+                              int stride, int accumulate, float* dx, int* err, void* stream);
+/* dw, db on the tensor cores (BF16 operands, FP32 accumulation; the voxels are split into
+ * fixed ranges whose partial sums are added in order).  work: the number of floats
+ * pf_cnn_conv3d_bwd_weight_tc_workspace returns for these sizes; db may be NULL. */
+size_t pf_cnn_conv3d_bwd_weight_tc_workspace(int N, int Cin, int X, int Y, int Z, int Cout, int stride);
+int pf_cnn_conv3d_bwd_weight_tc(const float* x, const float* dy, int N, int Cin, int X, int Y, int Z, int Cout,
+                                int stride, float* dw, float* db, float* work, int* err, void* stream);
 size_t pf_cnn_conv3d_bwd_weight_workspace(int Cin, int Cout); /* floats */
 int pf_cnn_conv3d_bwd_weight_f32(const float* x, const float* dy, int N, int Cin, int X, int Y, int Z, int Cout,
                                  int stride, float* dw, float* db, float* work, void* stream);

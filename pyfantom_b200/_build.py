@@ -25,6 +25,26 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompil
          "-I" + INCLUDE]
 
 
+def _cutlass_include():
+    """CuTe/CUTLASS headers vendored in the Python environment (used only to check the
+    tensor-core descriptor encodings at run time); None if absent."""
+    try:
+        import importlib.util
+        spec = importlib.util.find_spec("flashinfer")
+        if spec and spec.origin:
+            d = os.path.join(os.path.dirname(spec.origin), "data", "cutlass", "include")
+            if os.path.exists(os.path.join(d, "cute", "arch", "mma_sm100_desc.hpp")):
+                return d
+    except Exception:
+        pass
+    return None
+
+
+_CUTLASS = _cutlass_include()
+if _CUTLASS:
+    FLAGS.append("-I" + _CUTLASS)
+
+
 def nvcc() -> str:
     cand = [os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc"), shutil.which("nvcc") or ""]
     for c in cand:

@@ -113,6 +113,10 @@ SIGNATURES = {
     "pf_pgd_project_f64": (_I, [_LL, _P, _P, _D, _D, _D, _D, _P, _P, _P, _P]),
     "pf_cnn_conv3d_fwd_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P]),
     "pf_cnn_conv3d_bwd_data_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P]),
+    "pf_cnn_conv3d_fwd_tc": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _P]),
+    "pf_cnn_conv3d_bwd_data_tc": (_I, [_P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _P]),
+    "pf_cnn_conv3d_bwd_weight_tc_workspace": (_SZ, [_I, _I, _I, _I, _I, _I, _I]),
+    "pf_cnn_conv3d_bwd_weight_tc": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
     "pf_cnn_conv3d_bwd_weight_workspace": (_SZ, [_I, _I]),
     "pf_cnn_conv3d_bwd_weight_f32": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P]),
     "pf_cnn_relu_bwd_f32": (_I, [_LL, _P, _P, _P]),

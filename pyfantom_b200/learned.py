@@ -59,8 +59,11 @@ def _p(t):
 class WarmStartNet:
     """The U-Net, its flat float32 parameters, Adam state and activation buffers."""
 
-    def __init__(self, channels=(16, 32, 64, 48), seed: int = 0):
+    def __init__(self, channels=(16, 32, 64, 48), seed: int = 0, tensor_cores: bool = True):
         c1, c2, c3, c4 = (int(c) for c in channels)
+        # convolutions on the tensor cores (BF16 operands, FP32 accumulation) or on the
+        # CUDA cores in FP32 (the exact path the gradient checks use)
+        self.tensor_cores = bool(tensor_cores)
         self.channels = (c1, c2, c3, c4)
         # name, Cin, Cout, stride, relu
         self.layers = [
@@ -93,7 +96,16 @@ class WarmStartNet:
         wmax = max(co * ci for _, ci, co, _, _ in self.layers)
         self._wwork = torch.empty(int(_lib.load().pf_cnn_conv3d_bwd_weight_workspace(wmax, 1)), dtype=torch.float32,
                                   device=dev)
+        self._tc_err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._tc_work = {}
         self._bufs = {}
+
+    def tensor_core_errors(self):
+        """Number of tensor-core convolutions that gave up waiting since the last call
+        (0 in normal operation; their outputs were not written).  Reads one device int."""
+        e = int(self._tc_err.item())
+        self._tc_err.zero_()
+        return e
 
     # ---- parameters -----------------------------------------------------------------
     def w(self, name):
@@ -108,9 +120,9 @@ class WarmStartNet:
         np.savez(path, params=self.params.cpu().numpy(), channels=np.array(self.channels))
 
     @classmethod
-    def load(cls, path=DEFAULT_WEIGHTS):
+    def load(cls, path=DEFAULT_WEIGHTS, tensor_cores: bool = True):
         z = np.load(path)
-        net = cls(channels=tuple(int(c) for c in z["channels"]))
+        net = cls(channels=tuple(int(c) for c in z["channels"]), tensor_cores=tensor_cores)
         if z["params"].shape[0] != net.n_params:
             raise ValueError("weight file does not match the architecture")
         net.params.copy_(torch.from_numpy(z["params"]))
@@ -148,8 +160,13 @@ class WarmStartNet:
     def _conv(self, name, x, y):
         ci, co, s, r, _, _ = self.spec[name]
         N, _, X, Y, Z = x.shape
-        _lib.check(_lib.load().pf_cnn_conv3d_fwd_f32(_p(x), N, ci, X, Y, Z, _p(self.w(name)), _p(self.b(name)), co, s,
-                                                     r, _p(y), _lib.stream()))
+        L = _lib.load()
+        if self.tensor_cores:
+            _lib.check(L.pf_cnn_conv3d_fwd_tc(_p(x), N, ci, X, Y, Z, _p(self.w(name)), _p(self.b(name)), co, s, r,
+                                              _p(y), _p(self._tc_err), _lib.stream()))
+        else:
+            _lib.check(L.pf_cnn_conv3d_fwd_f32(_p(x), N, ci, X, Y, Z, _p(self.w(name)), _p(self.b(name)), co, s, r,
+                                               _p(y), _lib.stream()))
 
     def _up_cat(self, src, up, cat, c_off_skip, skip):
         """cat[:, :C] = up2(src), cat[:, c_off_skip:c_off_skip + Cskip] = skip."""
@@ -204,15 +221,29 @@ class WarmStartNet:
     def _wgrad(self, name, x, dy):
         ci, co, s, _, ow, ob = self.spec[name]
         N, _, X, Y, Z = x.shape
-        _lib.check(_lib.load().pf_cnn_conv3d_bwd_weight_f32(_p(x), _p(dy), N, ci, X, Y, Z, co, s, _p(self.grad[ow:ob]),
-                                                            _p(self.grad[ob:ob + co]), _p(self._wwork),
-                                                            _lib.stream()))
+        L = _lib.load()
+        if self.tensor_cores:
+            key = (name, N, X, Y, Z)
+            if key not in self._tc_work:
+                n = int(L.pf_cnn_conv3d_bwd_weight_tc_workspace(N, ci, X, Y, Z, co, s))
+                self._tc_work[key] = torch.empty(n, dtype=torch.float32, device=device())
+            _lib.check(L.pf_cnn_conv3d_bwd_weight_tc(_p(x), _p(dy), N, ci, X, Y, Z, co, s, _p(self.grad[ow:ob]),
+                                                     _p(self.grad[ob:ob + co]), _p(self._tc_work[key]),
+                                                     _p(self._tc_err), _lib.stream()))
+        else:
+            _lib.check(L.pf_cnn_conv3d_bwd_weight_f32(_p(x), _p(dy), N, ci, X, Y, Z, co, s, _p(self.grad[ow:ob]),
+                                                      _p(self.grad[ob:ob + co]), _p(self._wwork), _lib.stream()))
 
     def _dgrad(self, name, dy, xshape, dx, accumulate=0):
         ci, co, s, _, _, _ = self.spec[name]
         N, _, X, Y, Z = xshape
-        _lib.check(_lib.load().pf_cnn_conv3d_bwd_data_f32(_p(dy), N, ci, X, Y, Z, _p(self.w(name)), co, s, accumulate,
-                                                          _p(dx), _lib.stream()))
+        L = _lib.load()
+        if self.tensor_cores:
+            _lib.check(L.pf_cnn_conv3d_bwd_data_tc(_p(dy), N, ci, X, Y, Z, _p(self.w(name)), co, s, accumulate,
+                                                   _p(dx), _p(self._tc_err), _lib.stream()))
+        else:
+            _lib.check(L.pf_cnn_conv3d_bwd_data_f32(_p(dy), N, ci, X, Y, Z, _p(self.w(name)), co, s, accumulate,
+                                                    _p(dx), _lib.stream()))
 
     def _relu_bwd(self, y, dy):
         _lib.check(_lib.load().pf_cnn_relu_bwd_f32(y.numel(), _p(y), _p(dy), _lib.stream()))
@@ -365,6 +396,8 @@ class WarmStartNet:
                 lr_k = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * k / total))
                 self.adam(lr=lr_k)
             hist.append(float(losses[ep * steps * per:(ep + 1) * steps * per].mean()))
+            if self.tensor_cores and self.tensor_core_errors():
+                raise RuntimeError("a tensor-core convolution gave up waiting during this epoch")
             if log is not None:
                 log(f"epoch {ep + 1}/{epochs} loss {hist[-1]:.5f} ({time.time() - t0:.1f} s)")
         return hist

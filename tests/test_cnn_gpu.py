@@ -70,6 +70,60 @@ def test_conv_forward_and_adjoints(stride, shape, co):
     assert relerr(db, gb) < 1e-5
 
 
+def bf16(a):
+    """a rounded to BF16 (round to nearest even), back as float64."""
+    return torch.as_tensor(np.asarray(a, np.float32)).to(torch.bfloat16).double().numpy()
+
+
+@pytest.mark.parametrize("stride", [1, 2])
+@pytest.mark.parametrize("shape,co", [((2, 3, 5, 6, 7), 10), ((1, 16, 8, 8, 8), 16), ((3, 9, 4, 3, 6), 3),
+                                      ((1, 8, 17, 9, 13), 64), ((2, 160, 4, 4, 8), 48), ((1, 32, 16, 8, 8), 32)])
+def test_conv_tensor_core_kernels(stride, shape, co):
+    """The tcgen05 implicit-GEMM kernels (forward, input gradient, weight gradient): equal to
+    the oracle's convolution of the BF16-rounded operands to FP32 summation accuracy (1e-5
+    of the largest entry), and to the FP32 convolution within BF16 rounding (1e-2).  Shapes
+    cover K = 27 Cin not a multiple of the 16-wide MMA step (Cin 3, 9) or the 64-wide chunk,
+    output channels padded up to 16 (3, 10, 48), several 128-row tiles with a ragged last
+    one, weight gradients over several voxel ranges, and both strides."""
+    rng = np.random.default_rng(stride * 1000 + co + shape[1])
+    N, ci, X, Y, Z = shape
+    x, w, b = normal32(rng, shape), normal32(rng, (co, ci, 3, 3, 3)), normal32(rng, co)
+    xt, wt, bt = f32(x), f32(w), f32(b)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ref_r = C.conv3d(bf16(x), bf16(w), b, stride)
+    ref = C.conv3d(x, w, b, stride)
+    y = torch.full(ref.shape, float("nan"), dtype=torch.float32, device="cuda")
+    for relu in (0, 1):
+        _lib.check(lib().pf_cnn_conv3d_fwd_tc(P(xt), N, ci, X, Y, Z, P(wt), P(bt), co, stride, relu, P(y), P(err),
+                                              S()))
+        assert int(err.item()) == 0
+        assert relerr(y, np.maximum(ref_r, 0) if relu else ref_r) < 1e-5
+        assert relerr(y, np.maximum(ref, 0) if relu else ref) < 1e-2
+    dy = normal32(rng, ref.shape)
+    dyt = f32(dy)
+    dx = torch.full(shape, float("nan"), dtype=torch.float32, device="cuda")
+    _lib.check(lib().pf_cnn_conv3d_bwd_data_tc(P(dyt), N, ci, X, Y, Z, P(wt), co, stride, 0, P(dx), P(err), S()))
+    assert int(err.item()) == 0
+    gx_r = C.conv3d_bwd_data(bf16(dy), bf16(w), shape, stride)
+    assert relerr(dx, gx_r) < 1e-5
+    assert relerr(dx, C.conv3d_bwd_data(dy, w, shape, stride)) < 1e-2
+    _lib.check(lib().pf_cnn_conv3d_bwd_data_tc(P(dyt), N, ci, X, Y, Z, P(wt), co, stride, 1, P(dx), P(err), S()))
+    assert relerr(dx, 2 * gx_r) < 1e-5
+    # weight gradient: split over voxel ranges, ranges summed in order
+    nwork = int(lib().pf_cnn_conv3d_bwd_weight_tc_workspace(N, ci, X, Y, Z, co, stride))
+    work = torch.empty(nwork, dtype=torch.float32, device="cuda")
+    dw = torch.full((co, ci, 3, 3, 3), float("nan"), dtype=torch.float32, device="cuda")
+    db = torch.full((co,), float("nan"), dtype=torch.float32, device="cuda")
+    _lib.check(lib().pf_cnn_conv3d_bwd_weight_tc(P(xt), P(dyt), N, ci, X, Y, Z, co, stride, P(dw), P(db), P(work),
+                                                 P(err), S()))
+    assert int(err.item()) == 0
+    gw_r, _ = C.conv3d_bwd_weight(bf16(x), bf16(dy), stride)
+    assert relerr(dw, gw_r) < 1e-5
+    assert relerr(db, bf16(dy).sum(axis=(0, 2, 3, 4))) < 1e-5
+    gw, _ = C.conv3d_bwd_weight(x, dy, stride)
+    assert relerr(dw, gw) < 1e-2
+
+
 def test_conv_rejects_bad_stride():
     t = torch.zeros(8, device="cuda")
     assert lib().pf_cnn_conv3d_fwd_f32(P(t), 1, 1, 2, 2, 2, P(t), P(t), 1, 3, 0, P(t), S()) == _lib.PF_BAD_ARG
@@ -213,8 +267,13 @@ def test_energy_loss_kernel():
     assert 0.0 <= float(loss) <= 1.0
 
 
-def test_network_gradient_matches_oracle():
-    net = learned.WarmStartNet(channels=(4, 4, 8, 8), seed=3)
+@pytest.mark.parametrize("tc", [False, True])
+def test_network_gradient_matches_oracle(tc):
+    """The composed U-Net loss and parameter gradient against the float64 oracle: 1e-4 with
+    the FP32 convolutions; with the tensor-core convolutions (BF16 operands) the loss to 1e-2
+    and each layer's gradient to 5e-2 of its largest entry."""
+    net = learned.WarmStartNet(channels=(4, 4, 8, 8), seed=3, tensor_cores=tc)
+    tl, tg = (1e-2, 5e-2) if tc else (1e-5, 1e-4)
     rng = np.random.default_rng(4)
     N, X, Y, Z = 2, 8, 8, 16
     x = normal32(rng, (N, 8, X, Y, Z))
@@ -225,21 +284,22 @@ def test_network_gradient_matches_oracle():
     W = {n: net.w(n).double().cpu().numpy().reshape(net.spec[n][1], net.spec[n][0], 3, 3, 3) for n in net.spec}
     B = {n: net.b(n).double().cpu().numpy() for n in net.spec}
     ref_loss, dW, dB = C.unet_loss_grad(W, B, x, t)
-    assert abs(float(loss) - ref_loss) < 1e-5 * ref_loss
+    assert abs(float(loss) - ref_loss) < tl * ref_loss
     g = net.grad.double().cpu().numpy()
     for n in net.spec:
         ci, co, _, _, ow, ob = net.spec[n]
-        assert relerr(g[ow:ob], dW[n].reshape(-1)) < 1e-4, n
-        assert relerr(g[ob:ob + co], dB[n]) < 1e-4, n
+        assert relerr(g[ow:ob], dW[n].reshape(-1)) < tg, n
+        assert relerr(g[ob:ob + co], dB[n]) < tg, n
     # single-sample path (upsampling straight into the concatenation)
     x1, t1 = f32(x[:1]), f32(t[:1].reshape(1, -1))
     net.loss_and_grad(x1, t1, loss)
     ref_loss, dW, dB = C.unet_loss_grad(W, B, x[:1], t[:1])
     g = net.grad.double().cpu().numpy()
-    assert abs(float(loss) - ref_loss) < 1e-5 * ref_loss
+    assert abs(float(loss) - ref_loss) < tl * ref_loss
     for n in ("c1a", "c4a", "d3", "out"):
         ci, co, _, _, ow, ob = net.spec[n]
-        assert relerr(g[ow:ob], dW[n].reshape(-1)) < 1e-4, n
+        assert relerr(g[ow:ob], dW[n].reshape(-1)) < tg, n
+    assert not tc or net.tensor_core_errors() == 0
 
 
 def test_training_reduces_loss():
