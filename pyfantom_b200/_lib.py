@@ -69,6 +69,7 @@ SIGNATURES = {
     "pf_status_string": (ctypes.c_char_p, [_I]),
     "pf_op_create": (_I, [ctypes.POINTER(pf_grid), _P, ctypes.POINTER(_P)]),
     "pf_op_destroy": (_I, [_P]),
+    "pf_op_set_variant": (_I, [_P, _I]),
     "pf_pack_mask": (_I, [_P, _P, _P, _P]),
     "pf_matvec_f64": (_I, [_P, _P, _P, _P, _P, _P]),
     "pf_matvec_f32": (_I, [_P, _P, _P, _P, _P, _P]),

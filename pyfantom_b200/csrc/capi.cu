@@ -99,6 +99,7 @@ extern "C" int pf_op_create(const pf_grid* grid, const double* h_K0, pf_op** out
     op->grid = g;
     memset(op->K0, 0, sizeof(op->K0));
     memcpy(op->K0, h_K0, sizeof(double) * nd * nd);
+    op->variant = 0;
     if ((s = op_factorise(op))) {
         delete h;
         return s;
@@ -169,6 +170,12 @@ extern "C" int pf_matvec_f32(const pf_op* op, const float* E, const float* u, co
     e.out = y;
     e.omega_scale = 1.0;
     return launch_fine_matvec<float, float>(op, E, u, node_mask, e, as_stream(stream));
+}
+
+extern "C" int pf_op_set_variant(pf_op* op, int variant) {
+    if (!op || variant < 0 || variant > 1) return fail(PF_BAD_ARG, "pf_op_set_variant: variant must be 0 or 1");
+    op->variant = variant;
+    return PF_OK;
 }
 
 extern "C" int pf_matvec_f32_bf16(const pf_op* op, const uint16_t* E_bf16, const float* u, const uint8_t* node_mask,

@@ -164,6 +164,51 @@ __device__ __forceinline__ T elem_scale(TE e) {
         return (T)e;
 }
 
+// Two FP32 values in one 64-bit register pair, operated on by the packed FP32 instructions
+// of sm_100 (add/sub/mul/fma .f32x2): the paired fine matvec below runs the element
+// operator on two z-neighbouring elements at once (x = the lower element, y = the upper).
+// (Its own namespace, so that its fma is found by argument-dependent lookup and does not
+// hide the scalar fma of the other kernels in this namespace.)
+namespace pk {
+struct F2 {
+    unsigned long long v;
+    __device__ __forceinline__ F2() {}
+    __device__ __forceinline__ explicit F2(float s) { asm("mov.b64 %0, {%1, %1};" : "=l"(v) : "f"(s)); }
+    __device__ __forceinline__ F2(float a, float b) { asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(a), "f"(b)); }
+    __device__ __forceinline__ float x() const {
+        float a, b;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+        return a;
+    }
+    __device__ __forceinline__ float y() const {
+        float a, b;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+        return b;
+    }
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+    F2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+    F2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+    F2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) {
+    F2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+}  // namespace pk
+using pk::F2;
+
 // Element operator in the Walsh basis.  glo / ghi: transformed lower / upper faces (yz
 // stages done); e: the element's scale.  Returns in G the lower-face outputs plus the
 // upper-face outputs of the previous element (carry), and leaves this element's upper-face
@@ -486,6 +531,211 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// 3D matvec, FP32, two elements per lane (paired register x-march)
+// ---------------------------------------------------------------------------------------
+// As k_matvec_h8r, but lane l of a warp computes the two z-neighbouring elements of columns
+// ka = kz0 - 1 + 2l and kb = ka + 1, and reads the node columns ka and kb of its two node rows.
+// Every value of the element operator is a pair (element ka, element kb) held in one 64-bit
+// register pair and computed by the packed FP32 instructions, so one instruction stream
+// serves two elements; the z butterfly needs one shuffle per pair (the next lane's column
+// ka is this lane's column kb + 1), the z neighbour on the way back one more, and the row
+// exchange moves two nodes per lane.  Lane l < 31 owns node columns kb and kb + 1 of row
+// je + 1 (lane 31 none: its upper element's z neighbour lies in the next tile), 62 per warp.
+// Cube elements (CM 2) only: the element's scale is folded into the seven coefficients.
+constexpr int kZTileP = 62;
+
+template <typename TE, int NW, int MINB, int MODE, bool DOT>
+__global__ void __launch_bounds__(NW * 32, MINB)
+    k_matvec_h8p(int NX, int NY, int NZ, int CXc, const float* __restrict__ u, const TE* __restrict__ E,
+                 const uint8_t* __restrict__ mask, const H8Coef<float> cfs, Epi<float> epi) {
+    pdl_wait();
+    pdl_trigger();
+    constexpr int TY = NW - 1, NT = NW * 32;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ float2 s_q[2][3][NW][32];
+    __shared__ double s_red[NW];
+    if (epi.skip && *epi.skip) return;
+    constexpr int mode = MODE;
+    constexpr bool need_b = mode != PF_EPI_STORE, need_x = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
+    constexpr bool need_xa = mode == PF_EPI_JACOBI_ADD;
+    const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int kz0 = blockIdx.x * kZTileP, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
+    const int je = jy0 - 1 + w;
+    const int ka = kz0 - 1 + 2 * l, kb = ka + 1;  // node columns (and element columns) of this lane
+    const bool oka = ka >= 0 && ka < nz, okb = kb < nz;  // kb >= kz0 >= 0
+    const bool r0 = je >= 0 && je < ny, r1 = je + 1 < ny;
+    const bool erow = je >= 0 && je < NY;
+    const bool eA = erow && ka >= 0 && ka < NZ;
+    const bool eB = l < 31 && erow && kb < NZ;
+    const bool own_row = w < TY && je + 1 < ny;
+    const bool ownb = own_row && l < 31 && kb < nz;
+    const bool ownn = own_row && l < 31 && kb + 1 < nz;
+    const int rows = nz * nx;
+    const int base0 = rows * je, base1 = base0 + rows;  // node (row, plane 0, column 0)
+    const int eplane = NY * NZ;
+    const int ebase = je * NZ;
+    const bool has_mask = mask != nullptr;
+    const float wgt = epi_omega(epi);
+    double dot = 0.0;
+    H8Coef<F2> cf;
+#pragma unroll
+    for (int q = 0; q < 7; q++) cf.c[q] = F2(cfs.c[q]);
+
+    // node values of columns ka, kb in rows je, je+1 of plane p (zero outside the mesh)
+    auto load = [&](int p, float (&va)[2][3], float (&vb)[2][3], int (&m)[2][2]) {
+        const bool pok = p >= 0 && p < nx;
+        const int pa0 = base0 + nz * p + ka, pa1 = base1 + nz * p + ka;
+        m[0][0] = m[0][1] = m[1][0] = m[1][1] = 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            va[0][c] = (pok && r0 && oka) ? u[3 * pa0 + c] : 0.f;
+            vb[0][c] = (pok && r0 && okb) ? u[3 * (pa0 + 1) + c] : 0.f;
+            va[1][c] = (pok && r1 && oka) ? u[3 * pa1 + c] : 0.f;
+            vb[1][c] = (pok && r1 && okb) ? u[3 * (pa1 + 1) + c] : 0.f;
+        }
+        if (has_mask) {
+            if (pok && r0 && oka) m[0][0] = mask[pa0];
+            if (pok && r0 && okb) m[0][1] = mask[pa0 + 1];
+            if (pok && r1 && oka) m[1][0] = mask[pa1];
+            if (pok && r1 && okb) m[1][1] = mask[pa1 + 1];
+        }
+    };
+    // transformed face of both elements: y stage per column, z stage with the pair's upper
+    // columns (kb, next lane's ka)
+    auto face = [&](float (&va)[2][3], float (&vb)[2][3], const int (&m)[2][2], F2 (&g)[3][2][2]) {
+        if (__any_sync(FULL, m[0][0] | m[0][1] | m[1][0] | m[1][1])) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if ((m[0][0] >> c) & 1) va[0][c] = 0.f;
+                if ((m[0][1] >> c) & 1) vb[0][c] = 0.f;
+                if ((m[1][0] >> c) & 1) va[1][c] = 0.f;
+                if ((m[1][1] >> c) & 1) vb[1][c] = 0.f;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const F2 v0(va[0][c], vb[0][c]), v1(va[1][c], vb[1][c]);
+            const F2 sm = v1 + v0, df = v1 - v0;
+            const float sa_n = __shfl_down_sync(FULL, sm.x(), 1), da_n = __shfl_down_sync(FULL, df.x(), 1);
+            const F2 sn(sm.y(), sa_n), dn(df.y(), da_n);
+            g[c][0][0] = sm + sn;
+            g[c][0][1] = sn - sm;
+            g[c][1][0] = df + dn;
+            g[c][1][1] = dn - df;
+        }
+    };
+    auto escale = [&](int ie) -> F2 {
+        const bool ok = ie >= 0 && ie < NX;
+        const int e = ebase + eplane * ie;
+        const float a = (ok && eA) ? elem_scale<float>(E[e + ka]) : 0.f;
+        const float b = (ok && eB) ? elem_scale<float>(E[e + kb]) : 0.f;
+        return F2(a, b);
+    };
+
+    F2 carry[3][2][2];
+    auto step = [&](int s, F2 (&gl)[3][2][2], F2 (&gh)[3][2][2], float (&va)[2][3], float (&vb)[2][3],
+                    int (&m)[2][2], F2& e) {
+        const int ie = ix0 - 1 + s;
+        face(va, vb, m, gh);
+        if (s < CXc) load(ie + 2, va, vb, m);
+        const bool out_now = s >= 1 && ie < nx;
+        const int nob = base1 + nz * ie + kb;  // owned nodes nob (column kb) and nob + 1
+        F2 G[3][2][2];
+        h8_element<F2, 2>(gl, gh, e, cf, nullptr, carry, G);
+        e = (s < CXc) ? escale(ie + 1) : F2(0.f);
+        // epilogue operands of the owned nodes, loaded after the element operator (held
+        // across it they would spill), consumed after the barrier
+        float pb[2][3], px[2][3], pd[2][3], pa[2][3], pt[2][3];
+        int mo[2] = {0, 0};
+        if (out_now) {
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const bool own = q == 0 ? ownb : ownn;
+                if (!own) continue;
+                const int no = nob + q;
+                if (has_mask) mo[q] = mask[no];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    if constexpr (need_b) pb[q][c] = epi.b[3 * no + c];
+                    if constexpr (need_x) px[q][c] = epi.x[3 * no + c];
+                    if constexpr (need_x) pd[q][c] = epi.dinv[3 * no + c];
+                    if constexpr (need_xa) pa[q][c] = epi.xadd[3 * no + c];
+                    if constexpr (DOT) pt[q][c] = epi.dot_a[3 * no + c];
+                }
+            }
+        }
+        // inverse y and z stages: node kb = (lower element's upper z) + (upper element's lower
+        // z); node kb + 1 = (upper element's upper z) + (next lane's lower element's lower z)
+        float P1[2][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const F2 r0a = G[c][0][0] - G[c][1][0], r0b = G[c][0][1] - G[c][1][1];
+            const F2 r1a = G[c][0][0] + G[c][1][0], r1b = G[c][0][1] + G[c][1][1];
+            const F2 lo0 = r0a - r0b, up0 = r0a + r0b, lo1 = r1a - r1b, up1 = r1a + r1b;
+            P1[0][c] = up1.x() + lo1.y();
+            P1[1][c] = up1.y() + __shfl_down_sync(FULL, lo1.x(), 1);
+            const float q0 = up0.x() + lo0.y();
+            const float q1 = up0.y() + __shfl_down_sync(FULL, lo0.x(), 1);
+            s_q[s & 1][c][w][l] = make_float2(q0, q1);
+        }
+        __syncthreads();
+        if (out_now) {
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const bool own = q == 0 ? ownb : ownn;
+                if (!own) continue;
+                const int no = nob + q;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float2 sq = s_q[s & 1][c][w + 1][l];
+                    float y = P1[q][c] + (q == 0 ? sq.x : sq.y);
+                    if ((mo[q] >> c) & 1) y = u[3 * no + c];
+                    float o = y;
+                    if constexpr (mode == PF_EPI_RESID) {
+                        o = pb[q][c] - y;
+                    } else if constexpr (mode == PF_EPI_JACOBI) {
+                        o = px[q][c] + wgt * pd[q][c] * (pb[q][c] - y);
+                    } else if constexpr (mode == PF_EPI_JACOBI_ADD) {
+                        o = pa[q][c] + px[q][c] + wgt * pd[q][c] * (pb[q][c] - y);
+                    }
+                    epi.out[3 * no + c] = o;
+                    if constexpr (DOT) dot += (double)pt[q][c] * (double)(epi.dot_of_y ? y : o);
+                }
+            }
+        }
+    };
+
+    F2 gA[3][2][2], gB[3][2][2];
+    float vA[2][3], vB[2][3];
+    int mk[2][2];
+    load(ix0 - 1, vA, vB, mk);
+    face(vA, vB, mk, gA);
+    load(ix0, vA, vB, mk);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) carry[c][a][b] = F2(0.f);
+    F2 eP = escale(ix0 - 1);
+    for (int s = 0; s <= CXc; s++) {
+        step(s, gA, gB, vA, vB, mk, eP);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int b = 0; b < 2; b++) gA[c][a][b] = gB[c][a][b];
+    }
+    if constexpr (DOT) {
+        const double sblk = block_sum<NT>(dot, s_red);
+        if (threadIdx.x == 0)
+            epi.dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = sblk;
+    }
+}
+
 template <typename T>
 static H8Blk<T> make_blk(const Op* op) {
     H8Blk<T> b;
@@ -528,6 +778,29 @@ long long h8_num_blocks(const Grid& g, int fp32) {
     h8r_launch_dims(g, fp32 != 0, &gr, &cx);
     return (long long)gr.x * gr.y * gr.z;
 }
+
+// paired FP32 kernel: 12 warps (11 owned node rows), 1 block per SM (up to 168 registers:
+// at 2 blocks x 8 warps the 128-register cap spilled), 62 owned columns
+constexpr int kNWp = 12, kMinBp = 1;
+static void h8p_launch_dims(const Grid& g, dim3* grid, int* CXc) {
+    const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
+    const int tz = (nz + kZTileP - 1) / kZTileP, ty = (ny + kNWp - 2) / (kNWp - 1);
+    const long long slots = (long long)kNumSM * kMinBp;
+    const long long cols = (long long)tz * ty;
+    int best = 4;
+    long long best_cost = -1;
+    for (int cx = 4; cx <= 64; cx++) {
+        const long long nb = cols * ((nx + cx - 1) / cx);
+        const long long cost = ((nb + slots - 1) / slots) * (cx + 1);
+        if (best_cost < 0 || cost <= best_cost) {
+            best_cost = cost;
+            best = cx;
+        }
+    }
+    *CXc = best;
+    *grid = dim3(tz, ty, (nx + best - 1) / best);
+}
+static bool use_paired(const Op* op) { return op->grid.dim == 3 && op->cube && op->variant == 0; }
 
 // ---------------------------------------------------------------------------------------
 // 2D matvec (node gather, dense 8x8 K0)
@@ -629,10 +902,59 @@ static int h8r_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* 
 #undef PF_H8R
 }
 
+template <typename TE, int MODE, bool DOT>
+static int h8p_launch(dim3 grid, int cx, const Grid& g, const float* u, const TE* E, const uint8_t* mask,
+                      const H8Coef<float>& cf, const Epi<float>& epi, cudaStream_t st) {
+    PF_CUDA(launch_pdl(k_matvec_h8p<TE, kNWp, kMinBp, MODE, DOT>, dim3(grid), dim3(kNWp * 32), 0, st, g.nel[0],
+                       g.nel[1], g.nel[2], cx, u, E, mask, cf, epi));
+    return PF_OK;
+}
+
+template <typename TE>
+static int h8p_dispatch(const Op* op, const TE* E, const float* u, const uint8_t* mask, const Epi<float>& epi,
+                        cudaStream_t st) {
+    const Grid& g = op->grid;
+    H8Coef<float> cf;
+    for (int q = 0; q < 33; q++) cf.c[q] = 0.f;
+    const double* v = op->cube_v;
+    const double vals[7] = {v[0] - v[1], v[1], v[2], v[3], v[4], v[5] - v[6], v[6]};
+    for (int q = 0; q < 7; q++) cf.c[q] = (float)vals[q];
+    dim3 grid;
+    int cx;
+    h8p_launch_dims(g, &grid, &cx);
+    pf::count_launch();
+    const bool dot = epi.dot_partial != nullptr;
+#define PF_H8P(M, D) return h8p_launch<TE, M, D>(grid, cx, g, u, E, mask, cf, epi, st)
+    switch (epi.mode) {
+        case PF_EPI_STORE:
+            if (dot) PF_H8P(PF_EPI_STORE, true);
+            PF_H8P(PF_EPI_STORE, false);
+        case PF_EPI_RESID:
+            if (dot) PF_H8P(PF_EPI_RESID, true);
+            PF_H8P(PF_EPI_RESID, false);
+        case PF_EPI_JACOBI:
+            if (dot) PF_H8P(PF_EPI_JACOBI, true);
+            PF_H8P(PF_EPI_JACOBI, false);
+        default:
+            if (dot) PF_H8P(PF_EPI_JACOBI_ADD, true);
+            PF_H8P(PF_EPI_JACOBI_ADD, false);
+    }
+#undef PF_H8P
+}
+
 template <typename T, typename TE>
 int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mask, const Epi<T>& epi,
                        cudaStream_t st) {
     const Grid& g = op->grid;
+    if constexpr (sizeof(T) == 4) {
+        if (use_paired(op)) {
+            if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");
+            const int s = h8p_dispatch<TE>(op, E, u, mask, epi, st);
+            if (s) return s;
+            PF_LAUNCH_CHECK("fine matvec launch");
+            return PF_OK;
+        }
+    }
     if (g.dim == 3) {
         // a cube element's seven values (a-b, b, c, d, e, f-g, g), the 33 nonzeros of another
         // isotropic box, or (CM 0) the dense class blocks
@@ -671,6 +993,12 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
 }
 
 long long fine_matvec_num_blocks(const Op* op, int fp32) {
+    if (fp32 && use_paired(op)) {
+        dim3 gr;
+        int cx;
+        h8p_launch_dims(op->grid, &gr, &cx);
+        return (long long)gr.x * gr.y * gr.z;
+    }
     return op->grid.dim == 3 ? h8_num_blocks(op->grid, fp32) : q4_num_blocks(op->grid);
 }
 

@@ -29,6 +29,7 @@ struct pf_op {
     double coef[33];
     int sparse, cube;
     double cube_v[7];
+    int variant;  // FP32 fine matvec of cube elements: 0 two elements per lane (packed), 1 one
 };
 
 namespace pf {

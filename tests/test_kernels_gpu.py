@@ -412,3 +412,49 @@ def test_guess_select_picks_lower_energy(lib):
         want = (best @ f) / q * best if q > 0 else np.zeros(n)
         assert rel(N(out), want) < 1e-12
         assert N(work)[-3] == (1.0 if best is xb else 0.0)
+
+
+@pytest.mark.parametrize("nel", [(5, 13, 61), (7, 12, 62), (9, 3, 63), (4, 23, 124), (70, 11, 125), (3, 2, 1),
+                                 (13, 22, 186), (40, 12, 60)])
+@pytest.mark.parametrize("variant", [0, 1])
+def test_matvec_fp32_variants_tile_edges(lib, nel, variant):
+    """Both FP32 fine matvecs of cube elements (variant 0: two elements per thread in packed
+    FP32, 62 owned node columns per warp and 11 owned node rows per block; variant 1: one
+    element per thread) on grids around their tile edges (nz + 1 = 62, 63, 64, 125, 126,
+    187), with constraints on a tenth of the DOFs, against the oracle, and bitwise
+    repeatable."""
+    rng = np.random.default_rng(sum(nel) + 17 * variant)
+    op = Op(lib, nel)
+    lib.check(lib.load().pf_op_set_variant(op.h, variant))
+    E = rng.uniform(1e-3, 1.0, int(np.prod(nel))).astype(np.float32)
+    u = rng.standard_normal(op.ndof).astype(np.float32)
+    cons = rng.choice(op.ndof, size=max(1, op.ndof // 10), replace=False)
+    ref = O.matvec(nel, op.K0, E, u, cons)
+    y = op.matvec(E, u, cons, fp32=True)
+    assert rel(y, ref) < 2e-5
+    assert rel(op.matvec(E, u, None, fp32=True), O.matvec(nel, op.K0, E, u)) < 2e-5
+    assert np.array_equal(op.matvec(E, u, cons, fp32=True), y)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_vcycle_fp32_variants_match(lib, variant):
+    """The mixed-precision V-cycle (Jacobi, residual and correction epilogues of the FP32
+    fine matvec) with either FP32 kernel agrees with the FP64 V-cycle to FP32 accuracy."""
+    from pyfantom_b200 import workloads
+    from pyfantom_b200.CUDA import MultiGrid, StructuredMesh3D, StructuredStiffnessKernel
+    from pyfantom_b200.physics import LinearElasticity
+    nel = (32, 16, 64)
+    wl = workloads.cantilever3d(*nel)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
+        kern = StructuredStiffnessKernel(mesh)
+        lib.check(lib.load().pf_op_set_variant(kern._op, variant))
+        kern.add_constraints(torch.as_tensor(wl["fixed_dofs"], device="cuda"))
+        kern.set_rho(torch.as_tensor(wl["E"], device="cuda"))
+        sol = MultiGrid(mesh, kern, maxiter=100, tol=1e-8, n_smooth=2, omega=0.6, n_level=3, precision=prec)
+        sol.setup()
+        r = np.random.default_rng(1).standard_normal(kern.shape[0])
+        r[wl["fixed_dofs"]] = 0.0
+        out[prec] = sol.vcycle(torch.as_tensor(r, device="cuda"), omega=0.45).cpu().numpy()
+    assert rel(out["mixed"], out["fp64"]) < 1e-4
