@@ -141,6 +141,15 @@ int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega, void* stre
  * Blocks the calling thread until the solve ends; info is filled on return. */
 int pf_mg_solve(pf_mg* mg, const double* b, double* x, int use_x0, double tol, int maxiter,
                 pf_solve_info* info, void* stream);
+/* Deflation space of the following pf_mg_solve calls (a learned coarse-grid correction): Q =
+ * the three displacement components of the nodal field y (n DOFs, zero at constrained DOFs),
+ * W = K Q.  PCG starts from x0 = x + Q G^-1 Q^T (b - K x), G = Q^T W, and removes
+ * Q G^-1 W^T z from each preconditioned residual z (deflated PCG of Saad, Yeung, Erhel and
+ * Guyomarc'h, SIAM J. Sci. Comput. 21 (2000)); the V-cycle is unchanged.  Components whose
+ * G diagonal is zero are left out.  Requires pf_mg_setup; each pf_mg_setup clears it (K Q
+ * changes with the densities).  y = NULL clears it.  No reference counterpart: the
+ * reference's MultiGrid.solve (_solvers.py:573-660) has no coarse-space deflation. */
+int pf_mg_set_deflation(pf_mg* mg, const double* y, void* stream);
 /* y = A_l u with the operator the V-cycle applies on level l in [0, n_level) (l = 0: the
  * fine matvec; l = 1: the element-level operator or the stencil; deeper: the stencil), in
  * the V-cycle precision (double for precision 0, float otherwise).  Requires pf_mg_setup. */

@@ -60,6 +60,9 @@ def lib():
             "or_mgcg_solve_timed": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                    _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, _ip, _dp]),
+            "or_mgcg_solve_deflated": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                      _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, _dp, _ip]),
             "or_cg_solve": (ctypes.c_int, [ctypes.c_int, _ip, _dp, _dp, _bp, _dp, _dp, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_int, _dp]),
             "or_mg_vcycle": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -213,8 +216,10 @@ def stencil_to_dense(nel, A):
 
 
 def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega=0.4, omega_boost=1.06,
-               tol=1e-8, maxiter=1000, x0=None):
-    """MultiGrid-preconditioned CG with the reference CUDA semantics.
+               tol=1e-8, maxiter=1000, x0=None, deflation=None):
+    """MultiGrid-preconditioned CG with the reference CUDA semantics.  ``deflation``: a
+    nodal field whose components span a deflation space of the PCG (the library's learned
+    coarse-grid correction, pf_mg_set_deflation; no reference counterpart).
 
     Returns (x, iterations, relative recursive residual, status)."""
     dim = len(nel)
@@ -227,9 +232,15 @@ def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega
     x = np.zeros(nd) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
     res = ctypes.c_double(0.0)
     st = ctypes.c_int(0)
-    it = lib().or_mgcg_solve(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
-                             pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None),
-                             ctypes.byref(res), ctypes.byref(st))
+    if deflation is not None:
+        ya, py = _d(deflation)
+        it = lib().or_mgcg_solve_deflated(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
+                                          pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None), py,
+                                          ctypes.byref(res), ctypes.byref(st))
+    else:
+        it = lib().or_mgcg_solve(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
+                                 pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None),
+                                 ctypes.byref(res), ctypes.byref(st))
     return x, int(it), float(res.value), int(st.value)
 
 

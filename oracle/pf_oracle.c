@@ -614,12 +614,83 @@ static double wall_s(void) {
 #endif
 }
 
-/* or_mgcg_solve with wall-clock seconds of the hierarchy setup (times_out[0]) and of the
- * PCG start plus iterations (times_out[1]); times_out may be NULL */
-int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
-                        double omega_boost, double tol, int maxiter, const double* K0, const double* w,
-                        const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
-                        int* status_out, double* times_out) {
+/* Deflation space of the PCG (the library's learned coarse-grid correction, which has no
+ * reference counterpart): Q has one column per displacement component c, Q[i][c] = Y[i]
+ * where i % dim == c and DOF i is free, else 0; W = A Q, G = Q^T W.  The 3x3 (2x2) G is
+ * inverted on the components whose diagonal exceeds 1e-12 of the largest; the others get
+ * zero rows and columns.  Deflated PCG of Saad, Yeung, Erhel and Guyomarc'h (SIAM J. Sci.
+ * Comput. 21, 2000):  x0 = x + Q G^-1 Q^T (b - A x);  p = z - Q G^-1 W^T z + beta p. */
+typedef struct {
+    int on, dim;
+    long n;
+    double *Q, *W; /* dim columns of n */
+    double Gi[9];
+} defl_t;
+
+static void defl_build(defl_t* d, mg_t* m, const double* Y) {
+    memset(d, 0, sizeof(*d));
+    if (!Y) return;
+    const int dim = m->dim;
+    const long n = m->ndof[0];
+    d->on = 1;
+    d->dim = dim;
+    d->n = n;
+    d->Q = (double*)calloc((size_t)dim * n, sizeof(double));
+    d->W = (double*)calloc((size_t)dim * n, sizeof(double));
+    for (long i = 0; i < n; i++)
+        if (!(m->con && m->con[i])) d->Q[(i % dim) * n + i] = Y[i];
+    for (int c = 0; c < dim; c++) level_matvec(m, 0, d->Q + c * n, d->W + c * n);
+    double G[3][3], A[3][3], I[3][3];
+    int act[3] = {0, 0, 0};
+    double gmax = 0.0;
+    for (int c = 0; c < dim; c++)
+        for (int e = 0; e < dim; e++) G[c][e] = dot(n, d->Q + c * n, d->W + e * n);
+    for (int c = 0; c < dim; c++) gmax = fmax(gmax, G[c][c]);
+    for (int c = 0; c < dim; c++) act[c] = gmax > 0.0 && G[c][c] > 1e-12 * gmax;
+    for (int c = 0; c < dim; c++)
+        for (int e = 0; e < dim; e++) {
+            A[c][e] = (act[c] && act[e]) ? 0.5 * (G[c][e] + G[e][c]) : (c == e ? 1.0 : 0.0);
+            I[c][e] = c == e ? 1.0 : 0.0;
+        }
+    for (int k = 0; k < dim; k++) { /* Gauss-Jordan, SPD */
+        const double piv = A[k][k];
+        for (int j = 0; j < dim; j++) {
+            A[k][j] /= piv;
+            I[k][j] /= piv;
+        }
+        for (int i = 0; i < dim; i++)
+            if (i != k) {
+                const double f = A[i][k];
+                for (int j = 0; j < dim; j++) {
+                    A[i][j] -= f * A[k][j];
+                    I[i][j] -= f * I[k][j];
+                }
+            }
+    }
+    for (int c = 0; c < 3; c++)
+        for (int e = 0; e < 3; e++) d->Gi[c * 3 + e] = (c < dim && e < dim && act[c] && act[e]) ? I[c][e] : 0.0;
+}
+
+/* v -= Q G^-1 (M^T u)  (M = Q or W) when sign < 0, v += ... when sign > 0 */
+static void defl_apply(const defl_t* d, const double* M, const double* u, double* v, double sign) {
+    const long n = d->n;
+    double t[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+    for (int k = 0; k < d->dim; k++) t[k] = dot(n, M + k * n, u);
+    for (int k = 0; k < d->dim; k++)
+        for (int j = 0; j < d->dim; j++) c[k] += d->Gi[k * 3 + j] * t[j];
+    for (int k = 0; k < d->dim; k++)
+        for (long i = 0; i < n; i++) v[i] += sign * c[k] * d->Q[k * n + i];
+}
+
+static void defl_free(defl_t* d) {
+    free(d->Q);
+    free(d->W);
+}
+
+static int mgcg_core(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                     double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                     const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
+                     int* status_out, double* times_out, const double* Y) {
     mg_t m;
     const double t0 = wall_s();
     int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con);
@@ -636,10 +707,18 @@ int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, doub
         double *r = (double*)malloc(sizeof(double) * n), *z = (double*)malloc(sizeof(double) * n);
         double *p = (double*)malloc(sizeof(double) * n), *q = (double*)malloc(sizeof(double) * n);
         if (!use_x0) memset(x, 0, sizeof(double) * n);
+        defl_t D;
+        defl_build(&D, &m, Y);
         level_matvec(&m, 0, x, q);
         for (long i = 0; i < n; i++) r[i] = rhs[i] - q[i];
+        if (D.on) {
+            defl_apply(&D, D.Q, r, x, 1.0);
+            level_matvec(&m, 0, x, q);
+            for (long i = 0; i < n; i++) r[i] = rhs[i] - q[i];
+        }
         vcycle(&m, 0, z, r, cur);
         memcpy(p, z, sizeof(double) * n);
+        if (D.on) defl_apply(&D, D.W, z, p, -1.0);
         double rho_old = dot(n, r, z);
         double norm_b = sqrt(dot(n, rhs, rhs));
         status = 1;
@@ -664,9 +743,11 @@ int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, doub
             double beta = rho_new / rho_old;
 #pragma omp parallel for
             for (long i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+            if (D.on) defl_apply(&D, D.W, z, p, -1.0);
             rho_old = rho_new;
         }
         free(r); free(z); free(p); free(q);
+        defl_free(&D);
     }
     if (times_out) {
         times_out[0] = t1 - t0;
@@ -676,6 +757,25 @@ int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, doub
     *res_out = R;
     *status_out = status;
     return iters;
+}
+
+/* or_mgcg_solve with wall-clock seconds of the hierarchy setup (times_out[0]) and of the
+ * PCG start plus iterations (times_out[1]); times_out may be NULL */
+int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                        double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                        const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
+                        int* status_out, double* times_out) {
+    return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
+                     use_x0, res_out, status_out, times_out, NULL);
+}
+
+/* or_mgcg_solve with the deflation space spanned by the components of the nodal field Y */
+int or_mgcg_solve_deflated(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                           double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                           const uint8_t* con, const double* rhs, double* x, int use_x0, const double* Y,
+                           double* res_out, int* status_out) {
+    return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
+                     use_x0, res_out, status_out, NULL, Y);
 }
 
 int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,

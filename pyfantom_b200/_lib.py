@@ -65,6 +65,7 @@ SIGNATURES = {
     "pf_mg_profile_select": (_I, [_P, _I]),
     "pf_mg_level_matvec": (_I, [_P, _I, _P, _P, _P]),
     "pf_mg_level_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "pf_mg_set_deflation": (_I, [_P, _P, _P]),
     "pf_last_error": (ctypes.c_char_p, []),
     "pf_status_string": (ctypes.c_char_p, [_I]),
     "pf_op_create": (_I, [ctypes.POINTER(pf_grid), _P, ctypes.POINTER(_P)]),

@@ -36,6 +36,7 @@ struct PcgState {
     double tol, min_omega, d_omega;
     int it, maxiter, done, status;
     int stop_le;  // 1: stop when R <= tol (cupyx cg, plain CG); 0: R < tol (MultiGrid)
+    double coef[3];  // deflation: G^-1 Q^T r (start) or G^-1 W^T z (iterations)
 };
 
 struct Level {
@@ -67,6 +68,12 @@ struct pf_mg {
     const double* E = nullptr;
     const uint8_t* mask = nullptr;
     pf::CoarseOp* c1 = nullptr;     // element-level operator of level 1 (else its stencil)
+    // deflation by a coarse space Q = [q_0 q_1 q_2], q_c = a field's component c (learned
+    // coarse-grid correction): field, W = A Q (FP32) and G^-1 (FP64, 9 values + 3 flags)
+    int defl = 0;
+    float* yf = nullptr;
+    float* Wf = nullptr;
+    double* dG = nullptr;
     float* Ef = nullptr;            // FP32 element scales of the V-cycle (precision 1)
     __nv_bfloat16* Eb = nullptr;    // BF16 element scales of the V-cycle (precision 2)
     double *r = nullptr, *p = nullptr, *q = nullptr;
@@ -149,6 +156,9 @@ __device__ double sum_partials(const double* partials, long long np, double* s_r
     return block_sum<kRedThreads>(s, s_red);
 }
 
+__device__ void defl_coef(const double* partials, long long np, int off, const double* dG, PcgState* st,
+                          double* s_red);
+
 __global__ void __launch_bounds__(kRedThreads) k_pcg_normb(const double* partials, long long np, PcgState* st) {
     pdl_wait();
     pdl_trigger();
@@ -171,12 +181,14 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_normb(const double* partial
     }
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_pcg_rho0(const double* partials, long long np, PcgState* st) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_rho0(const double* partials, long long np, PcgState* st,
+                                                          const double* dG) {
     pdl_wait();
     pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double rz = sum_partials(partials, np, s_red);
+    if (dG) defl_coef(partials, np, 1, dG, st, s_red);  // G^-1 W^T z
     if (threadIdx.x == 0) {
         st->rho_old = rz;
         if (!isfinite(rz)) {
@@ -254,12 +266,14 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_check(const double* partial
     }
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_pcg_beta(const double* partials, long long np, PcgState* st) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_beta(const double* partials, long long np, PcgState* st,
+                                                          const double* dG) {
     pdl_wait();
     pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     if (st->done) return;
     const double rz = sum_partials(partials, np, s_red);
+    if (dG) defl_coef(partials, np, 1, dG, st, s_red);  // G^-1 W^T z
     if (threadIdx.x == 0) {
         if (!isfinite(rz)) {
             st->done = 1;
@@ -271,14 +285,23 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_beta(const double* partials
     }
 }
 
+// p = z + beta p (init: p = z); with the deflation field yf, z - Q coef in place of z
 template <typename TZ>
-__global__ void k_pcg_p(long long n, const TZ* __restrict__ z, double* __restrict__ p, const PcgState* st, int init) {
+__global__ void k_pcg_p(long long n, const TZ* __restrict__ z, double* __restrict__ p, const PcgState* st, int init,
+                        const float* __restrict__ yf, int dof) {
     pdl_wait();
     pdl_trigger();
     if (st->done) return;
     const double b = st->beta;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        p[i] = init ? (double)z[i] : (double)z[i] + b * p[i];
+    const double c0 = st->coef[0], c1 = st->coef[1], c2 = st->coef[2];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double zi = (double)z[i];
+        if (yf) {
+            const int c = (int)(i % dof);
+            zi -= (double)yf[i] * (c == 0 ? c0 : c == 1 ? c1 : c2);
+        }
+        p[i] = init ? zi : zi + b * p[i];
+    }
 }
 
 __global__ void k_f2d(long long n, const float* __restrict__ a, double* __restrict__ b) {
@@ -286,6 +309,160 @@ __global__ void k_f2d(long long n, const float* __restrict__ a, double* __restri
     pdl_trigger();
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
+}
+
+// ---------------------------------------------------------------------------------------
+// deflation (learned coarse-grid correction): PCG on the complement of span(Q) in the
+// energy inner product (Saad, Yeung, Erhel, Guyomarc'h, SIAM J. Sci. Comput. 21 (2000)):
+//   x0 = x + Q G^-1 Q^T (b - A x),  r0 = b - A x0,   G = Q^T A Q = Q^T W,
+//   z = M r,  p = z - Q G^-1 W^T z (+ beta p),
+// with the V-cycle M unchanged.  Q has three columns: the components of one nodal field
+// (zero on constrained DOFs; DOF i is component i % dof, a third column is zero in 2D); G is
+// inverted on the components whose diagonal is positive.
+// ---------------------------------------------------------------------------------------
+__global__ void k_defl_field(long long n, int dof, const double* __restrict__ y, const uint8_t* __restrict__ mask,
+                             float* __restrict__ yf) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const bool con = mask && ((mask[i / dof] >> (int)(i % dof)) & 1);
+        yf[i] = con ? 0.f : (float)y[i];
+    }
+}
+__global__ void k_defl_comp(long long n, int dof, const float* __restrict__ yf, int c, double* __restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (int)(i % dof) == c ? (double)yf[i] : 0.0;
+}
+// partials of G_cd = q_c . W_d (9 per block, index c*3 + d, stride gridDim.x)
+__global__ void __launch_bounds__(kRedThreads) k_defl_gram(long long n, int dof, const float* __restrict__ yf,
+                                                           const float* __restrict__ Wf, double* partials) {
+    __shared__ double s_red[kRedThreads / 32];
+    double g[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) g[q] = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % dof);
+        const double y = yf[i];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double t = y * (double)Wf[d * n + i];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++)
+                if (cc == c) g[cc * 3 + d] += t;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const double t = block_sum<kRedThreads>(g[q], s_red);
+        if (threadIdx.x == 0) partials[(long long)q * gridDim.x + blockIdx.x] = t;
+    }
+}
+// G^-1 over the components with a positive diagonal (the others get zero rows and columns)
+__global__ void __launch_bounds__(kRedThreads) k_defl_ginv(const double* partials, long long np, double* dG) {
+    __shared__ double s_red[kRedThreads / 32];
+    double G[9];
+    for (int q = 0; q < 9; q++) G[q] = sum_partials(partials + q * np, np, s_red);
+    if (threadIdx.x != 0) return;
+    // symmetrise, select the active components
+    double A[3][3], I[3][3];
+    int act[3];
+    const double gmax = fmax(G[0], fmax(G[4], G[8]));
+    for (int c = 0; c < 3; c++) act[c] = G[c * 4] > 1e-12 * gmax && gmax > 0.0;
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) {
+            A[c][d] = (act[c] && act[d]) ? 0.5 * (G[c * 3 + d] + G[d * 3 + c]) : (c == d ? 1.0 : 0.0);
+            I[c][d] = c == d ? 1.0 : 0.0;
+        }
+    // Gauss-Jordan on the SPD 3x3 (no pivoting needed)
+    int ok = 1;
+    for (int k = 0; k < 3; k++) {
+        const double piv = A[k][k];
+        if (!(piv > 0.0)) {
+            ok = 0;
+            break;
+        }
+        for (int j = 0; j < 3; j++) {
+            A[k][j] /= piv;
+            I[k][j] /= piv;
+        }
+        for (int i = 0; i < 3; i++)
+            if (i != k) {
+                const double f = A[i][k];
+                for (int j = 0; j < 3; j++) {
+                    A[i][j] -= f * A[k][j];
+                    I[i][j] -= f * I[k][j];
+                }
+            }
+    }
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) dG[c * 3 + d] = (ok && act[c] && act[d]) ? I[c][d] : 0.0;
+}
+// partials of s_c = q_c . r (3 per block)
+__global__ void __launch_bounds__(kRedThreads) k_defl_qt(long long n, int dof, const double* __restrict__ r,
+                                                         const float* __restrict__ yf, double* partials) {
+    __shared__ double s_red[kRedThreads / 32];
+    double a[3] = {0.0, 0.0, 0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % dof);
+        const double t = (double)yf[i] * r[i];
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++)
+            if (cc == c) a[cc] += t;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const double t = block_sum<kRedThreads>(a[q], s_red);
+        if (threadIdx.x == 0) partials[(long long)q * gridDim.x + blockIdx.x] = t;
+    }
+}
+// st->coef = G^-1 (3 sums of partials starting at partials + off * np)
+__device__ void defl_coef(const double* partials, long long np, int off, const double* dG, PcgState* st,
+                          double* s_red) {
+    double t[3];
+    for (int q = 0; q < 3; q++) t[q] = sum_partials(partials + (off + q) * np, np, s_red);
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; c++) st->coef[c] = dG[c * 3] * t[0] + dG[c * 3 + 1] * t[1] + dG[c * 3 + 2] * t[2];
+}
+__global__ void __launch_bounds__(kRedThreads) k_defl_coef(const double* partials, long long np, const double* dG,
+                                                           PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ double s_red[kRedThreads / 32];
+    if (st->done) return;
+    defl_coef(partials, np, 0, dG, st, s_red);
+}
+// x += Q coef
+__global__ void k_defl_xadd(long long n, int dof, const float* __restrict__ yf, double* __restrict__ x,
+                            const PcgState* st) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) return;
+    const double c0 = st->coef[0], c1 = st->coef[1], c2 = st->coef[2];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % dof);
+        x[i] += (double)yf[i] * (c == 0 ? c0 : c == 1 ? c1 : c2);
+    }
+}
+// partials of r.z (index 0) and t_d = W_d . z (indices 1..3)
+template <typename TZ>
+__global__ void __launch_bounds__(kRedThreads) k_dot_defl(long long n, const double* __restrict__ r,
+                                                          const TZ* __restrict__ z, const float* __restrict__ Wf,
+                                                          double* partials, const int* skip) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ double s_red[kRedThreads / 32];
+    if (skip && *skip) return;
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double zi = (double)z[i];
+        a[0] += r[i] * zi;
+        a[1] += (double)Wf[i] * zi;
+        a[2] += (double)Wf[n + i] * zi;
+        a[3] += (double)Wf[2 * n + i] * zi;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const double t = block_sum<kRedThreads>(a[q], s_red);
+        if (threadIdx.x == 0) partials[(long long)q * gridDim.x + blockIdx.x] = t;
+    }
 }
 
 static unsigned vec_blocks(long long n) {
@@ -445,7 +622,7 @@ static void mg_free(pf_mg* mg) {
     coarse_destroy(mg->c1);
     mg->c1 = nullptr;
     for (void* p : {(void*)mg->K0_dev, (void*)mg->Kc_dev, (void*)mg->elem_flag, (void*)mg->node_flag, (void*)mg->Ef,
-                    (void*)mg->Eb,
+                    (void*)mg->Eb, (void*)mg->yf, (void*)mg->Wf, (void*)mg->dG,
                     (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st,
                     (void*)mg->Eint, (void*)mg->bi, (void*)mg->xi})
         if (p) cudaFree(p);
@@ -455,6 +632,13 @@ static void mg_free(pf_mg* mg) {
     if (mg->ev_out) cudaEventDestroy(mg->ev_out);
     if (mg->cs) cudaStreamDestroy(mg->cs);
     if (mg->h_snap) cudaFreeHost(mg->h_snap);
+}
+
+// the captured start and iteration graphs bake in pointers and the PCG variant
+static void drop_graphs(pf_mg* mg) {
+    for (cudaGraphExec_t& gx : mg->g_start)
+        if (gx) cudaGraphExecDestroy(gx), gx = nullptr;
+    if (mg->g_chunk) cudaGraphExecDestroy(mg->g_chunk), mg->g_chunk = nullptr;
 }
 
 static int dalloc(void** p, size_t bytes) {
@@ -542,6 +726,7 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     if (mg->fp32 && fine_matvec_num_blocks(op, 1) > np) np = fine_matvec_num_blocks(op, 1);
     if (np < 8 * kNumSM) np = 8 * kNumSM;
     for (int l = 1; l < mg->nlev; l++) np = np > stencil_matvec_num_blocks(mg->L[l].g) ? np : stencil_matvec_num_blocks(mg->L[l].g);
+    if (np < 9LL * 8 * kNumSM) np = 9LL * 8 * kNumSM;  // the deflation's 9 sums per reduction block
     mg->npartials = np;
     s = s ? s : dalloc((void**)&mg->partials, np * sizeof(double));
     s = s ? s : dalloc((void**)&mg->st, sizeof(PcgState));
@@ -593,10 +778,10 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
     PF_CUDA(cudaMemcpyAsync(mg->Eint, E, sizeof(double) * mg->op->grid.n_elem, cudaMemcpyDeviceToDevice, st));
     E = mg->Eint;
     mg->E = E;
-    if (node_mask != mg->g_mask) {  // graphs bake the mask pointer in: recapture
-        for (cudaGraphExec_t& g : mg->g_start)
-            if (g) cudaGraphExecDestroy(g), g = nullptr;
-        if (mg->g_chunk) cudaGraphExecDestroy(mg->g_chunk), mg->g_chunk = nullptr;
+    if (node_mask != mg->g_mask) drop_graphs(mg);  // graphs bake the mask pointer in: recapture
+    if (mg->defl) {  // A Q changes with the densities: the deflation space is set again after setup
+        mg->defl = 0;
+        drop_graphs(mg);
     }
     mg->mask = node_mask;
     mg->ready = false;
@@ -645,11 +830,7 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
     if (mg->c1) {
         bool moved = false;
         if ((s = coarse_setup(mg->c1, E, node_mask, mg->elem_flag, mg->K0_dev, st, &moved))) return s;
-        if (moved) {  // the captured graphs hold the old dirty storage: recapture
-            for (cudaGraphExec_t& gx : mg->g_start)
-                if (gx) cudaGraphExecDestroy(gx), gx = nullptr;
-            if (mg->g_chunk) cudaGraphExecDestroy(mg->g_chunk), mg->g_chunk = nullptr;
-        }
+        if (moved) drop_graphs(mg);  // the captured graphs hold the old dirty storage: recapture
     }
     // coarsest: dense factor and inverse
     Dense& D = mg->dense;
@@ -726,15 +907,28 @@ static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaSt
         float* res;
         if ((s = vcycle<float>(mg, 0, (const float*)mg->L[0].b, &res, nullptr, nullptr, st))) return s;
         pf::count_launch();
-        PF_CUDA(launch_pdl(k_dot_partial<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, res, mg->partials, &mg->st->done));
+        if (mg->defl)  // r.z and W^T z
+            PF_CUDA(launch_pdl(k_dot_defl<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)mg->r,
+                               (const float*)res, (const float*)mg->Wf, mg->partials, (const int*)&mg->st->done));
+        else
+            PF_CUDA(launch_pdl(k_dot_partial<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, res, mg->partials, &mg->st->done));
         PF_LAUNCH_CHECK("dot launch");
         *z_out = res;
         *np_out = vec_blocks(n);
     } else {
         double* res;
-        if ((s = vcycle<double>(mg, 0, mg->r, &res, mg->partials, mg->r, st))) return s;
+        if (mg->defl) {
+            if ((s = vcycle<double>(mg, 0, mg->r, &res, nullptr, nullptr, st))) return s;
+            pf::count_launch();
+            PF_CUDA(launch_pdl(k_dot_defl<double>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)mg->r,
+                               (const double*)res, (const float*)mg->Wf, mg->partials, (const int*)&mg->st->done));
+            PF_LAUNCH_CHECK("dot launch");
+            *np_out = vec_blocks(n);
+        } else {
+            if ((s = vcycle<double>(mg, 0, mg->r, &res, mg->partials, mg->r, st))) return s;
+            *np_out = fine_matvec_num_blocks(mg->op, 0);
+        }
         *z_out = res;
-        *np_out = fine_matvec_num_blocks(mg->op, 0);
     }
     return PF_OK;
 }
@@ -743,9 +937,11 @@ static int update_p(pf_mg* mg, const void* z, int init, cudaStream_t st) {
     const long long n = mg->L[0].ndof;
     pf::count_launch();
     if (mg->fp32)
-        PF_CUDA(launch_pdl(k_pcg_p<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const float*)z, mg->p, mg->st, init));
+        PF_CUDA(launch_pdl(k_pcg_p<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const float*)z, mg->p, mg->st, init,
+                           (const float*)(mg->defl ? mg->yf : nullptr), mg->op->grid.dof));
     else
-        PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)z, mg->p, mg->st, init));
+        PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)z, mg->p, mg->st, init,
+                           (const float*)(mg->defl ? mg->yf : nullptr), mg->op->grid.dof));
     PF_LAUNCH_CHECK("p update launch");
     return PF_OK;
 }
@@ -772,7 +968,8 @@ static int pcg_iteration(pf_mg* mg, double* x, cudaStream_t st) {
     long long np;
     if ((s = precondition(mg, &z, &np, st, true))) return s;
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st));
+    PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st,
+                       (const double*)(mg->defl ? mg->dG : nullptr)));
     PF_LAUNCH_CHECK("beta launch");
     return update_p(mg, z, 0, st);
 }
@@ -814,11 +1011,25 @@ static int solve_start(pf_mg* mg, int use_x0, cudaStream_t st) {
     pf::count_launch();
     PF_CUDA(launch_pdl(k_pcg_normb, dim3(1), dim3(kRedThreads), 0, st, mg->partials, vec_blocks(n), mg->st));
     PF_LAUNCH_CHECK("pcg start");
+    if (mg->defl) {  // x += Q G^-1 Q^T r, r = b - A x
+        const unsigned vb = vec_blocks(n);
+        pf::count_launch(3);
+        PF_CUDA(launch_pdl(k_defl_qt, dim3(vb), dim3(kRedThreads), 0, st, n, mg->op->grid.dof, (const double*)mg->r,
+                           (const float*)mg->yf, mg->partials));
+        PF_CUDA(launch_pdl(k_defl_coef, dim3(1), dim3(kRedThreads), 0, st, (const double*)mg->partials, (long long)vb,
+                           (const double*)mg->dG, mg->st));
+        PF_CUDA(launch_pdl(k_defl_xadd, dim3(vb), dim3(kRedThreads), 0, st, n, mg->op->grid.dof, (const float*)mg->yf,
+                           mg->xi, (const PcgState*)mg->st));
+        PF_LAUNCH_CHECK("deflated start");
+        Epi<double> e = make_epi<double>(PF_EPI_RESID, mg->bi, nullptr, nullptr, nullptr, mg->r, nullptr, 1.0, nullptr);
+        if ((s = fine_mv<double>(mg, mg->xi, e, st))) return s;
+    }
     const void* z;
     long long np;
     if ((s = precondition(mg, &z, &np, st, false))) return s;
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st));
+    PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, mg->partials, np, mg->st,
+                       (const double*)(mg->defl ? mg->dG : nullptr)));
     return update_p(mg, z, 1, st);
 }
 
@@ -964,9 +1175,9 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
     pf::count_launch();
     PF_CUDA(launch_pdl(k_dot_partial<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, r, partials, skip));
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
+    PF_CUDA(launch_pdl(k_pcg_rho0, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S, (const double*)nullptr));
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, p, S, 1));
+    PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, p, S, 1, (const float*)nullptr, 3));
     PF_LAUNCH_CHECK("cg start");
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -991,9 +1202,9 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
             pf::count_launch();
             PF_CUDA(launch_pdl(k_pcg_check, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
             pf::count_launch();
-            PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S));
+            PF_CUDA(launch_pdl(k_pcg_beta, dim3(1), dim3(kRedThreads), 0, st, partials, vb, S, (const double*)nullptr));
             pf::count_launch();
-            PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, p, S, 0));
+            PF_CUDA(launch_pdl(k_pcg_p<double>, dim3(vb), dim3(kRedThreads), 0, st, n, r, p, S, 0, (const float*)nullptr, 3));
         }
         PF_LAUNCH_CHECK("cg iteration");
         it += chunk;
@@ -1019,8 +1230,48 @@ extern "C" int pf_cg_solve(const pf_op* op, const double* E, const uint8_t* node
 }
 
 // ---------------------------------------------------------------------------------------
-// profiling of the fine-level matvec inside a solve
+// deflation space: Q = the three components of a nodal field, W = A Q, G^-1 = (Q^T W)^-1
 // ---------------------------------------------------------------------------------------
+extern "C" int pf_mg_set_deflation(pf_mg* mg, const double* y, void* stream) {
+    if (!mg) return fail(PF_BAD_ARG, "pf_mg_set_deflation: NULL solver");
+    if (!y) {
+        if (mg->defl) drop_graphs(mg);  // the captured iterations are the deflated ones
+        mg->defl = 0;
+        return PF_OK;
+    }
+    if (!mg->ready) return fail(PF_BAD_ARG, "pf_mg_set_deflation: call pf_mg_setup first");
+    cudaStream_t st = as_stream(stream);
+    const long long n = mg->L[0].ndof;
+    int s = PF_OK;
+    if (!mg->yf) {
+        s = dalloc((void**)&mg->yf, (size_t)n * sizeof(float));
+        s = s ? s : dalloc((void**)&mg->Wf, (size_t)3 * n * sizeof(float));
+        s = s ? s : dalloc((void**)&mg->dG, 16 * sizeof(double));
+        if (s) return s;
+    }
+    const unsigned vb = vec_blocks(n);
+    pf::count_launch();
+    const int dof = mg->op->grid.dof;
+    k_defl_field<<<vb, kRedThreads, 0, st>>>(n, dof, y, mg->mask, mg->yf);
+    PF_LAUNCH_CHECK("deflation field launch");
+    if (dof == 2) PF_CUDA(cudaMemsetAsync(mg->Wf + 2 * n, 0, (size_t)n * sizeof(float), st));
+    for (int c = 0; c < dof; c++) {  // W_c = A q_c, through the FP64 fine matvec (q, p as scratch)
+        pf::count_launch();
+        k_defl_comp<<<vb, kRedThreads, 0, st>>>(n, dof, mg->yf, c, mg->q);
+        PF_LAUNCH_CHECK("deflation column launch");
+        Epi<double> e = make_epi<double>(PF_EPI_STORE, nullptr, nullptr, nullptr, nullptr, mg->p, nullptr, 1.0, nullptr);
+        if ((s = launch_fine_matvec<double, double>(mg->op, mg->E, mg->q, mg->mask, e, st))) return s;
+        if ((s = launch_d2f(n, mg->p, mg->Wf + (size_t)c * n, st))) return s;
+    }
+    pf::count_launch(2);
+    k_defl_gram<<<vb, kRedThreads, 0, st>>>(n, dof, mg->yf, mg->Wf, mg->partials);
+    k_defl_ginv<<<1, kRedThreads, 0, st>>>(mg->partials, (long long)vb, mg->dG);
+    PF_LAUNCH_CHECK("deflation Gram launch");
+    if (!mg->defl) drop_graphs(mg);  // the captured iterations are the plain ones
+    mg->defl = 1;
+    return PF_OK;
+}
+
 extern "C" int pf_mg_level_matvec(pf_mg* mg, int level, const void* u, void* y, void* stream) {
     if (!mg || !u || !y) return fail(PF_BAD_ARG, "pf_mg_level_matvec: NULL argument");
     if (!mg->ready) return fail(PF_BAD_ARG, "pf_mg_level_matvec: call pf_mg_setup first");
@@ -1043,6 +1294,9 @@ extern "C" int pf_mg_level_info(const pf_mg* mg, int* h_elem_level1, int* h_dirt
     return PF_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// profiling of the fine-level matvec inside a solve
+// ---------------------------------------------------------------------------------------
 extern "C" int pf_mg_set_profiling(pf_mg* mg, int max_launches) {
     if (!mg || max_launches < 0) return fail(PF_BAD_ARG, "pf_mg_set_profiling: bad argument");
     PF_CUDA(cudaDeviceSynchronize());

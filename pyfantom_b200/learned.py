@@ -583,3 +583,42 @@ class LearnedWarmStart:
             a, r = b["scale"][-2:].tolist()
             self.last = dict(alpha=a, residual=r)
         return b["x0"]
+
+
+class LearnedCoarseSpace:
+    """Learned coarse-grid correction of the MGCG (``MultiGrid(..., coarse_correction=...)``):
+    the network's predicted displacement field, interpolated to the mesh and zeroed on
+    constrained DOFs, spans a three-column deflation space Q (one column per displacement
+    component).  The solver starts from x0 = x + Q G^-1 Q^T (b - K x) with G = Q^T K Q, the
+    energy-optimal correction of its start inside span(Q), and keeps every search direction
+    K-orthogonal to Q (deflated PCG), so the part of the error the network predicts is
+    removed once and does not come back through the V-cycle.  ``pool`` as in
+    ``LearnedWarmStart``.  No counterpart in the reference."""
+
+    def __init__(self, net: WarmStartNet, pool: int = 1):
+        self.net = net
+        self.pool = int(pool)
+        self._scratch = {}
+
+    def field(self, kern, rhs):
+        """Nodal field (float64, one value per DOF) for K(rho) u = rhs with the kernel's
+        current rho and constraints."""
+        L = _lib.load()
+        n = rhs.shape[0]
+        key = (n, kern.nel)
+        if key not in self._scratch:
+            dev = device()
+            nel = kern.nel
+            P = self.pool
+            self._scratch = {key: dict(
+                y=torch.empty(n, dtype=torch.float64, device=dev),
+                feat=torch.empty((1, N_IN, nel[0] // P, nel[1] // P, nel[2] // P), dtype=torch.float32, device=dev),
+                work=torch.zeros(1, dtype=torch.int32, device=dev))}
+        b = self._scratch[key]
+        g = kern._grid
+        _lib.check(L.pf_cnn_features_f32(ctypes.byref(g), self.pool, _p(kern.rho), _p(rhs), kern._mask_ptr(),
+                                         _p(b["work"]), _p(b["feat"]), _lib.stream()))
+        nodes = self.net.predict_nodes(b["feat"])
+        _lib.check(L.pf_cnn_guess_f64(ctypes.byref(g), self.pool, _p(nodes), kern._mask_ptr(), _p(b["y"]),
+                                      _lib.stream()))
+        return b["y"]

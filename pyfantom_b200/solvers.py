@@ -14,7 +14,10 @@
   ``warm_start`` (an object with ``guess(kernel, rhs)``, e.g. learned.LearnedWarmStart,
   that supplies the initial guess of a solve that does not reuse ``last_x0``) and
   ``coarse_op`` ('element': level 1 applied element by element from the fine densities
-  when the element allows it, the default; 'stencil': assembled stencils on every level).
+  when the element allows it, the default; 'stencil': assembled stencils on every level)
+  and ``coarse_correction`` (an object with ``field(kernel, rhs)``, e.g.
+  learned.LearnedCoarseSpace, whose nodal field spans a deflation space of the PCG,
+  ``pf_mg_set_deflation``).
 
 ``solve(rhs, rho=None, use_last=True)`` returns ``(U, residual)`` like the reference;
 ``last_x0`` holds the warm start.  Solver statistics of the last call are in
@@ -146,9 +149,10 @@ class MultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="cholmod", matrix_free=False, low_level_tol=1e-8,
                  low_level_maxiter=5000, min_omega=0.4, omega_boost=1.06, *, precision="fp64", check_every=4,
-                 warm_start=None, coarse_op="element"):
+                 warm_start=None, coarse_op="element", coarse_correction=None):
         self.kernel = kernel
         self.warm_start = warm_start
+        self.coarse_correction = coarse_correction
         self.mesh = mesh
         self.last_x0 = None
         self.tol = tol
@@ -266,6 +270,9 @@ class MultiGrid(Solver):
         else:
             x = torch.empty(n, dtype=torch.float64, device=device())
         self.setup()
+        if self.coarse_correction is not None:
+            y = as_cuda(self.coarse_correction.field(k, rhs), torch.float64)
+            _lib.check(_lib.load().pf_mg_set_deflation(self._mg, _lib.ptr(y), _lib.stream()))
         info = _lib.pf_solve_info()
         _lib.check(_lib.load().pf_mg_solve(self._mg, _lib.ptr(rhs), _lib.ptr(x), int(warm), float(self.tol),
                                            int(self.maxiter), ctypes.byref(info), _lib.stream()))

@@ -218,3 +218,19 @@ def test_cg_stops_at_tolerance_and_solves():
     assert res_prev > 1e-9
     xm, _, _, _ = O.mgcg_solve(wl["nel"], K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=1, tol=1e-12)
     assert rel(x, xm) < 1e-7
+
+
+def test_oracle_deflated_pcg():
+    """The oracle's deflated PCG (the library's learned coarse-grid correction): with the
+    solution as the field it converges in one iteration; with a white-noise field it reaches
+    the plain solution to the same tolerance."""
+    nel = (16, 8, 8)
+    wl = workloads.cantilever3d(*nel)
+    K0 = unit_K0(3)
+    x, it, _, st = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=2, tol=1e-10)
+    assert st == 0
+    x1, it1, _, st1 = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=2, tol=1e-8, deflation=x)
+    assert st1 == 0 and it1 == 1 and rel(x1, x) < 1e-8
+    y = np.random.default_rng(0).standard_normal(x.size)
+    x2, it2, _, st2 = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=2, tol=1e-10, deflation=y)
+    assert st2 == 0 and abs(it2 - it) <= 3 and rel(x2, x) < 1e-8
