@@ -398,6 +398,8 @@ __global__ void __launch_bounds__(kRedThreads) k_defl_ginv(const double* partial
 // partials of s_c = q_c . r (3 per block)
 __global__ void __launch_bounds__(kRedThreads) k_defl_qt(long long n, int dof, const double* __restrict__ r,
                                                          const float* __restrict__ yf, double* partials) {
+    pdl_wait();  // r, and the partials the previous kernel reads
+    pdl_trigger();
     __shared__ double s_red[kRedThreads / 32];
     double a[3] = {0.0, 0.0, 0.0};
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
