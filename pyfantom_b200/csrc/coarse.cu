@@ -17,13 +17,16 @@
 // and no coefficient traffic, where the assembled stencil streams 126 coefficients per
 // coarse node.
 //
-// Coarse elements with a constrained fine node ("dirty": their Z-masked children and the
-// identity rows of I - Z) keep an explicit Walsh-basis matrix: every coefficient pair (I, J)
-// of the dirty part of A^ (the masked children of all dirty elements containing I and J,
-// plus the identity term) is assigned to the first dirty element (in element order) that
-// contains both I and J, so the dirty matrices sum to exactly that part.  A dirty element
-// is marked by Ehat_0 = -(index + 1) (Ehat_0 = sum E > 0 otherwise), confirmed against the
-// dirty list.
+// Coarse elements with a constrained fine node ("dirty": their Z-masked children) keep an
+// explicit Walsh-basis matrix: every coefficient pair (I, J) of the dirty part of A^ (the
+// masked children of all dirty elements containing I and J) is assigned to the first dirty
+// element (in element order) that contains both I and J, so the dirty matrices sum to
+// exactly that part.  A dirty element is marked by Ehat_0 = -(index + 1) (Ehat_0 = sum E > 0
+// otherwise), confirmed against the dirty list.  The identity rows Phat^T (I - Z) Phat are
+// applied per coarse node in the physical basis (27 neighbours per component) by the owner
+// of the node: inside a Walsh-basis matrix their O(1) entries would be mixed with the
+// O(E_min) stiffness of void children, which FP32 cannot resolve (SIMP densities reach
+// 1e-9 of the solid at a clamped face).
 //
 // The matvec is an x-march like the fine one (csrc/elemop.cu): warps cover element rows in
 // y, lanes element columns in z, the element's Walsh transform is formed from the two
@@ -227,8 +230,8 @@ __device__ __forceinline__ double hp(int d) { return d == 0 ? 1.0 : d == 1 ? 0.5
 // LI, LJ of dirty element dlist[d]: the dirty part of A^[I, J] if this element is the first
 // dirty element containing I and J, else 0.  The dirty part: every dirty element containing
 // I and J contributes sum_c E_c (Z Phat_c)^T K0 (Z Phat_c) (children with their fine
-// constraints masked), plus the identity rows P^T (I - Z) P of the constrained fine DOFs
-// (as the reference's level-0 Galerkin, mgm.cu:247-447).
+// constraints masked, as the reference's level-0 Galerkin, mgm.cu:247-447); the identity
+// rows are k_ident_rows'.
 __global__ void __launch_bounds__(64) k_dirty_blocks(GridC<3> gf, GridC<3> gc, const double* __restrict__ E,
                                                      const uint8_t* __restrict__ mask,
                                                      const uint8_t* __restrict__ elem_flag,
@@ -307,24 +310,45 @@ __global__ void __launch_bounds__(64) k_dirty_blocks(GridC<3> gf, GridC<3> gc, c
                         }
                     }
                 }
-        // identity rows of the constrained fine DOFs near both 2I and 2J
+    }
+    double* Md = M + (long long)d * 576;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) Md[(LI * 3 + a) * 24 + LJ * 3 + b] = blk[a * 3 + b];
+}
+
+// Identity rows of the level-1 Galerkin operator, Phat^T (I - Z) Phat: thread (q, o) writes,
+// for identity node n = nlist[q] and neighbour m = n + o (o = dx + 3 dy + 9 dz + 13), the
+// three per-component coefficients S[(a * 27 + o) * icap + q] = sum over the fine nodes f
+// within one fine spacing of both 2n and 2m whose DOF a is constrained of
+// 0.5^|f - 2n|_0 0.5^|f - 2m|_0 (the interpolation weights; mgm.cu:247-447 adds these rows).
+template <typename T>
+__global__ void k_ident_rows(GridC<3> gf, GridC<3> gc, const uint8_t* __restrict__ mask, const int* __restrict__ nlist,
+                             int nq, int icap, T* __restrict__ S) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nq * 27) return;
+    const int q = (int)(t / 27), o = (int)(t % 27);
+    const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+    const long long n = nlist[q];
+    const int nk = (int)(n % gc.nn[2]), ni = (int)((n / gc.nn[2]) % gc.nn[0]);
+    const int nj = (int)(n / ((long long)gc.nn[2] * gc.nn[0]));
+    const int mi = ni + dx, mj = nj + dy, mk = nk + dz;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (mi >= 0 && mj >= 0 && mk >= 0 && mi < gc.nn[0] && mj < gc.nn[1] && mk < gc.nn[2]) {
         for (int di = -1; di <= 1; di++)
             for (int dj = -1; dj <= 1; dj++)
                 for (int dk = -1; dk <= 1; dk++) {
-                    const int fi = 2 * I[0] + di, fj = 2 * I[1] + dj, fk = 2 * I[2] + dk;
+                    const int fi = 2 * ni + di, fj = 2 * nj + dj, fk = 2 * nk + dk;
                     if (fi < 0 || fj < 0 || fk < 0 || fi >= gf.nn[0] || fj >= gf.nn[1] || fk >= gf.nn[2]) continue;
-                    const int ei = fi - 2 * J[0], ej = fj - 2 * J[1], ek = fk - 2 * J[2];
+                    const int ei = fi - 2 * mi, ej = fj - 2 * mj, ek = fk - 2 * mk;
                     if (ei < -1 || ei > 1 || ej < -1 || ej > 1 || ek < -1 || ek > 1) continue;
                     const uint8_t m = mask[fnode(gf, fi, fj, fk)];
                     if (!m) continue;
                     const double w = hp((di != 0) + (dj != 0) + (dk != 0)) * hp((ei != 0) + (ej != 0) + (ek != 0));
                     for (int a = 0; a < 3; a++)
-                        if (m & (1 << a)) blk[a * 3 + a] += w;
+                        if (m & (1 << a)) acc[a] += w;
                 }
     }
-    double* Md = M + (long long)d * 576;
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++) Md[(LI * 3 + a) * 24 + LJ * 3 + b] = blk[a * 3 + b];
+    for (int a = 0; a < 3; a++) S[(long long)(a * 27 + o) * icap + q] = (T)acc[a];
 }
 
 // Walsh basis: W = T M T^T / 64, stored Wd[(i * 24 + j) * cap + d] (coalesced across the
@@ -439,11 +463,29 @@ __device__ __forceinline__ void coarse_element(const T (&glo)[3][2][2], const T 
     });
 }
 
+// identity rows of owned node (x, y, z), index q: sum over its 27 neighbours m of
+// S(a, m) (D u)_m per component a
+template <typename T>
+__device__ __forceinline__ void coarse_ident(int x, int y, int z, int nx, int ny, int nz, int q, int icap,
+                                             const T* __restrict__ S, const T* __restrict__ u, T (&out)[3]) {
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll 1
+    for (int o = 0; o < 27; o++) {
+        const int mx = x + o % 3 - 1, my = y + (o / 3) % 3 - 1, mz = z + o / 9 - 1;
+        if (mx < 0 || my < 0 || mz < 0 || mx >= nx || my >= ny || mz >= nz) continue;
+        const long long m = (long long)mz + (long long)nz * (mx + (long long)nx * my);
+        const T dm = inv_tw<T>(mx, nx) * inv_tw<T>(my, ny) * inv_tw<T>(mz, nz);
+        for (int a = 0; a < 3; a++) acc[a] = fma(S[(long long)(a * 27 + o) * icap + q], u[3 * m + a] * dm, acc[a]);
+    }
+    for (int a = 0; a < 3; a++) out[a] = acc[a];
+}
+
 template <typename T, int NW, int MINB, int MODE>
 __global__ void __launch_bounds__(NW * 32, MINB)
     k_coarse_matvec(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const T* __restrict__ Eh,
                     const T* __restrict__ Wd, const int* __restrict__ dlist, int cap, const CoarseCoef<T> cf,
-                    Epi<T> epi) {
+                    Epi<T> epi, const uint8_t* __restrict__ nflag, const int* __restrict__ nmap,
+                    const T* __restrict__ S, int icap) {
     pdl_wait();
     pdl_trigger();
     constexpr int TY = NW - 1;
@@ -541,9 +583,11 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         __syncthreads();
         if (out_now) {
             const T sc = so * inv_tw<T>(ie, nx);
+            T id[3] = {T(0), T(0), T(0)};
+            if (nflag && nflag[no]) coarse_ident<T>(ie, je + 1, kc + 1, nx, ny, nz, nmap[no], icap, S, u, id);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const T y = (P1[c] + s_q[s & 1][c][w + 1][l]) * sc;
+                const T y = (P1[c] + s_q[s & 1][c][w + 1][l] + id[c]) * sc;
                 T o = y;
                 if constexpr (MODE == PF_EPI_RESID) {
                     o = pb[c] - y;
@@ -605,11 +649,13 @@ static void coarse_launch_dims(const Grid& g, bool fp32, dim3* grid, int* CXc) {
 }
 
 template <typename T, int MODE>
-static int coarse_launch(dim3 grid, int cx, const Grid& g, const T* u, const T* Eh, const T* Wd, const int* dlist,
-                         int cap, const CoarseCoef<T>& cf, const Epi<T>& epi, cudaStream_t st) {
+static int coarse_launch(dim3 grid, int cx, const Grid& g, const T* u, const CoarseOp* c, const CoarseCoef<T>& cf,
+                         const Epi<T>& epi, cudaStream_t st) {
     constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
+    const uint8_t* nflag = c->nident > 0 ? c->nflag : nullptr;
     PF_CUDA(launch_pdl(k_coarse_matvec<T, kCNW, MINB, MODE>, grid, dim3(kCNW * 32), 0, st, g.nel[0], g.nel[1],
-                       g.nel[2], cx, u, Eh, Wd, dlist, cap, cf, epi));
+                       g.nel[2], cx, u, (const T*)c->Eh, (const T*)c->Wd, (const int*)c->dlist, c->cap, cf, epi,
+                       nflag, (const int*)c->nmap, (const T*)c->S, c->icap));
     return PF_OK;
 }
 
@@ -618,21 +664,19 @@ int launch_coarse_matvec(const CoarseOp* c, const Grid& g, const T* u, const Epi
     if (epi.dot_partial) return fail(PF_UNSUPPORTED, "coarse element matvec: no fused dot");
     CoarseCoef<T> cf;
     for (int q = 0; q < kCoarseCoefs; q++) cf.b[q] = (T)c->coef[q];
-    const T* Eh = (const T*)c->Eh;
-    const T* Wd = (const T*)c->Wd;
     dim3 grid;
     int cx;
     coarse_launch_dims(g, sizeof(T) == 4, &grid, &cx);
     pf::count_launch();
     switch (epi.mode) {
         case PF_EPI_STORE:
-            return coarse_launch<T, PF_EPI_STORE>(grid, cx, g, u, Eh, Wd, c->dlist, c->cap, cf, epi, st);
+            return coarse_launch<T, PF_EPI_STORE>(grid, cx, g, u, c, cf, epi, st);
         case PF_EPI_RESID:
-            return coarse_launch<T, PF_EPI_RESID>(grid, cx, g, u, Eh, Wd, c->dlist, c->cap, cf, epi, st);
+            return coarse_launch<T, PF_EPI_RESID>(grid, cx, g, u, c, cf, epi, st);
         case PF_EPI_JACOBI:
-            return coarse_launch<T, PF_EPI_JACOBI>(grid, cx, g, u, Eh, Wd, c->dlist, c->cap, cf, epi, st);
+            return coarse_launch<T, PF_EPI_JACOBI>(grid, cx, g, u, c, cf, epi, st);
         default:
-            return coarse_launch<T, PF_EPI_JACOBI_ADD>(grid, cx, g, u, Eh, Wd, c->dlist, c->cap, cf, epi, st);
+            return coarse_launch<T, PF_EPI_JACOBI_ADD>(grid, cx, g, u, c, cf, epi, st);
     }
 }
 template int launch_coarse_matvec<double>(const CoarseOp*, const Grid&, const double*, const Epi<double>&,
@@ -667,8 +711,9 @@ int coarse_create(const Op* op, int fp32, CoarseOp** out) {
     const long long ne = c->g.n_elem;
     s = calloc_dev(&c->Eh, (size_t)ne * 8 * c->tsize);
     s = s ? s : calloc_dev((void**)&c->dmap, (size_t)ne * sizeof(int));
-    s = s ? s : calloc_dev((void**)&c->count, sizeof(int));
-    if (!s && cudaMallocHost((void**)&c->h_count, sizeof(int)) != cudaSuccess) s = fail(PF_NO_MEMORY, "pinned alloc");
+    s = s ? s : calloc_dev((void**)&c->nmap, (size_t)c->g.n_nodes * sizeof(int));
+    s = s ? s : calloc_dev((void**)&c->count, 2 * sizeof(int));
+    if (!s && cudaMallocHost((void**)&c->h_count, 2 * sizeof(int)) != cudaSuccess) s = fail(PF_NO_MEMORY, "pinned alloc");
     if (s) {
         coarse_destroy(c);
         return s;
@@ -679,7 +724,8 @@ int coarse_create(const Op* op, int fp32, CoarseOp** out) {
 
 void coarse_destroy(CoarseOp* c) {
     if (!c) return;
-    for (void* p : {c->Eh, (void*)c->dmap, (void*)c->dlist, (void*)c->M, c->Wd, (void*)c->count})
+    for (void* p : {c->Eh, (void*)c->dmap, (void*)c->dlist, (void*)c->M, c->Wd, (void*)c->count, (void*)c->nmap,
+                    (void*)c->nlist, c->S})
         if (p) cudaFree(p);
     if (c->h_count) cudaFreeHost(c->h_count);
     delete c;
@@ -697,40 +743,60 @@ static GridC<3> gridc(const Grid& g) {
 // Ehat and the dirty matrices for densities E (FP64) and the fine node mask.  The dirty
 // list is recounted on every call; the host waits for the count (one int) and grows the
 // dirty storage when it no longer fits.
-int coarse_setup(CoarseOp* c, const double* E, const uint8_t* mask, const uint8_t* elem_flag, const double* K0_dev,
-                 cudaStream_t st, bool* realloc) {
+int coarse_setup(CoarseOp* c, const double* E, const uint8_t* mask, const uint8_t* elem_flag,
+                 const uint8_t* node_flag, const double* K0_dev, cudaStream_t st, bool* realloc) {
     *realloc = false;
     const Grid& gc = c->g;
     const long long ne = gc.n_elem;
-    if (ne >= (1LL << 31)) return fail(PF_BAD_ARG, "coarse grid too large");
-    int nd = 0;
+    if (ne >= (1LL << 31) || gc.n_nodes >= (1LL << 31)) return fail(PF_BAD_ARG, "coarse grid too large");
+    int nd = 0, ni = 0;
+    c->nflag = node_flag;
     if (mask) {
         for (int pass = 0; pass < 2; pass++) {
-            pf::count_launch();
+            pf::count_launch(2);
             k_dirty_scan<<<1, kScanThreads, 0, st>>>(ne, elem_flag, c->dmap, c->dlist, c->cap, c->count);
+            k_dirty_scan<<<1, kScanThreads, 0, st>>>(gc.n_nodes, node_flag, c->nmap, c->nlist, c->icap, c->count + 1);
             PF_LAUNCH_CHECK("dirty scan launch");
-            PF_CUDA(cudaMemcpyAsync(c->h_count, c->count, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(c->h_count, c->count, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
             PF_CUDA(cudaStreamSynchronize(st));
-            nd = *c->h_count;
-            if (nd <= c->cap) break;
+            nd = c->h_count[0];
+            ni = c->h_count[1];
+            if (nd <= c->cap && ni <= c->icap) break;
             if (nd >= (1 << 24)) return fail(PF_UNSUPPORTED, "coarse operator: %d dirty elements (limit 2^24)", nd);
-            for (void* p : {(void*)c->dlist, (void*)c->M, c->Wd})
-                if (p) cudaFree(p);
-            c->dlist = nullptr;
-            c->M = nullptr;
-            c->Wd = nullptr;
-            const int cap = nd + nd / 4 + 32;
-            int s = calloc_dev((void**)&c->dlist, (size_t)cap * sizeof(int));
-            s = s ? s : calloc_dev((void**)&c->M, (size_t)cap * 576 * sizeof(double));
-            s = s ? s : calloc_dev(&c->Wd, (size_t)cap * 576 * c->tsize);
-            if (s) {
-                c->cap = 0;
-                return s;
+            if (nd > c->cap) {
+                for (void* p : {(void*)c->dlist, (void*)c->M, c->Wd})
+                    if (p) cudaFree(p);
+                c->dlist = nullptr;
+                c->M = nullptr;
+                c->Wd = nullptr;
+                const int cap = nd + nd / 4 + 32;
+                int s = calloc_dev((void**)&c->dlist, (size_t)cap * sizeof(int));
+                s = s ? s : calloc_dev((void**)&c->M, (size_t)cap * 576 * sizeof(double));
+                s = s ? s : calloc_dev(&c->Wd, (size_t)cap * 576 * c->tsize);
+                if (s) {
+                    c->cap = 0;
+                    return s;
+                }
+                c->cap = cap;
             }
-            c->cap = cap;
+            if (ni > c->icap) {
+                for (void* p : {(void*)c->nlist, c->S})
+                    if (p) cudaFree(p);
+                c->nlist = nullptr;
+                c->S = nullptr;
+                const int icap = ni + ni / 4 + 32;
+                int s = calloc_dev((void**)&c->nlist, (size_t)icap * sizeof(int));
+                s = s ? s : calloc_dev(&c->S, (size_t)icap * 81 * c->tsize);
+                if (s) {
+                    c->icap = 0;
+                    return s;
+                }
+                c->icap = icap;
+            }
             *realloc = true;
         }
     }
+    c->nident = ni;
     c->ndirty = nd;
     const unsigned nb = (unsigned)((ne + 255) / 256);
     pf::count_launch();
@@ -751,6 +817,17 @@ int coarse_setup(CoarseOp* c, const double* E, const uint8_t* mask, const uint8_
         else
             k_dirty_walsh<double><<<nd, 576, 0, st>>>(c->M, c->cap, (double*)c->Wd);
         PF_LAUNCH_CHECK("dirty walsh launch");
+    }
+    if (ni > 0) {
+        pf::count_launch();
+        const unsigned nbi = (unsigned)(((long long)ni * 27 + 255) / 256);
+        if (c->tsize == 4)
+            k_ident_rows<float><<<nbi, 256, 0, st>>>(gridc(c->fine), gridc(gc), mask, c->nlist, ni, c->icap,
+                                                     (float*)c->S);
+        else
+            k_ident_rows<double><<<nbi, 256, 0, st>>>(gridc(c->fine), gridc(gc), mask, c->nlist, ni, c->icap,
+                                                      (double*)c->S);
+        PF_LAUNCH_CHECK("identity rows launch");
     }
     return PF_OK;
 }

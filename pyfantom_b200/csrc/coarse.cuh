@@ -15,9 +15,17 @@ struct CoarseOp {
     int* dlist = nullptr;         // dirty index -> coarse element
     double* M = nullptr;          // dirty matrices, physical basis, FP64 [cap][576]
     void* Wd = nullptr;           // dirty matrices, Walsh basis [576][cap], V-cycle precision
-    int* count = nullptr;         // device: number of dirty elements
+    int* count = nullptr;         // device: number of dirty elements, number of identity nodes
     int* h_count = nullptr;       // pinned copy
     int cap = 0, ndirty = 0;
+    // identity rows R (I - Z) P of the constrained fine DOFs, applied per coarse node in the
+    // physical basis (kept out of the Walsh-basis dirty matrices, where their O(1) entries
+    // would swamp the O(E_min) stiffness of void elements in FP32)
+    const uint8_t* nflag = nullptr;  // coarse node touches a constrained fine node
+    int* nmap = nullptr;             // coarse node -> identity index or -1
+    int* nlist = nullptr;            // identity index -> coarse node
+    void* S = nullptr;               // [3 * 27][icap] coefficients, V-cycle precision
+    int icap = 0, nident = 0;
 };
 
 // PF_OK if K0 has the structure of an isotropic box element (coefficients in coef[150])
@@ -25,8 +33,8 @@ int coarse_factorise(const Op* op, double* coef);
 int coarse_create(const Op* op, int fp32, CoarseOp** out);
 void coarse_destroy(CoarseOp* c);
 // Ehat and the dirty matrices for E; *realloc set when the dirty storage moved
-int coarse_setup(CoarseOp* c, const double* E, const uint8_t* mask, const uint8_t* elem_flag, const double* K0_dev,
-                 cudaStream_t st, bool* realloc);
+int coarse_setup(CoarseOp* c, const double* E, const uint8_t* mask, const uint8_t* elem_flag,
+                 const uint8_t* node_flag, const double* K0_dev, cudaStream_t st, bool* realloc);
 template <typename T>
 int launch_coarse_matvec(const CoarseOp* c, const Grid& g, const T* u, const Epi<T>& epi, cudaStream_t st);
 

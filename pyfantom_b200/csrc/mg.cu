@@ -831,7 +831,7 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
     }
     if (mg->c1) {
         bool moved = false;
-        if ((s = coarse_setup(mg->c1, E, node_mask, mg->elem_flag, mg->K0_dev, st, &moved))) return s;
+        if ((s = coarse_setup(mg->c1, E, node_mask, mg->elem_flag, mg->node_flag, mg->K0_dev, st, &moved))) return s;
         if (moved) drop_graphs(mg);  // the captured graphs hold the old dirty storage: recapture
     }
     // coarsest: dense factor and inverse

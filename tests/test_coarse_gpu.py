@@ -74,6 +74,40 @@ def test_level1_element_operator_equals_stencil(nel, kind, cons):
     assert rel(y32, yo) < 2e-5
 
 
+@pytest.mark.parametrize("kind", ["cantilever", "bridge", "random"])
+def test_level1_row_accuracy_at_simp_contrast(kind):
+    """SIMP contrast (solid 1, void 1e-9, void everywhere next to the constraints): every
+    row of the operator to 1e-5 (FP32) and 1e-12 (FP64) of that row's |A1| |u|, the accuracy
+    an assembled FP32 stencil has.  The identity rows of constrained fine DOFs are O(1) where
+    the void stiffness is O(1e-9); mixed into one Walsh-basis element matrix they would leave
+    the void rows of the FP32 operator with errors of order one."""
+    nel = (16, 8, 12)
+    rng = np.random.default_rng(17)
+    wl = workloads.cantilever3d(*nel) if kind != "bridge" else workloads.bridge3d(*nel)
+    cons = wl["fixed_dofs"]
+    if kind == "random":
+        n_nodes = int(np.prod(np.array(nel) + 1))
+        cons = np.unique(rng.choice(3 * n_nodes, size=n_nodes // 6, replace=False))
+    ex = np.repeat(np.arange(nel[0]), nel[1] * nel[2])  # element order: x slowest
+    E = np.where(rng.uniform(size=int(np.prod(nel))) < 0.5, 1e-9, 1.0)
+    if kind != "random":
+        E[ex <= 1] = 1e-9  # void at and next to the clamped face / supports
+        E[ex >= nel[0] - 2] = 1e-9
+    cnel = tuple(n // 2 for n in nel)
+    nc = int(np.prod(np.array(cnel) + 1)) * 3
+    A1 = O.galerkin_l0(nel, unit_K0(3), E, cons)
+    u = rng.standard_normal(nc).astype(np.float32).astype(np.float64)
+    yo = O.stencil_matvec(cnel, A1, u)
+    scale = O.stencil_matvec(cnel, np.abs(A1), np.abs(u))
+    s64, _ = _solver(nel, E, cons, 2)
+    assert s64.level_info()[0] and s64.level_info()[1] > 0
+    y64 = s64.level_matvec(1, torch.as_tensor(u, device="cuda")).cpu().numpy()
+    assert np.max(np.abs(y64 - yo) / scale) < 1e-12
+    s32, _ = _solver(nel, E, cons, 2, precision="mixed")
+    y32 = s32.level_matvec(1, torch.as_tensor(u, dtype=torch.float32, device="cuda")).cpu().numpy()
+    assert np.max(np.abs(y32 - yo) / scale) < 1e-5
+
+
 def test_level1_repeated_setup_and_growing_dirty_set():
     """Setups with new densities and a larger constraint set (the dirty storage grows and
     the solver's captured iterations are rebuilt): the operator follows each change."""
