@@ -6,13 +6,16 @@ Headline workload (default ``cantilever_256x128x128``): 256x128x128 H8 cantileve
 Gaussian-smoothed (sigma=2); MultiGrid-preconditioned CG with 5 coarse levels, 2 pre/post
 damped-Jacobi sweeps (omega=0.6, reference adaptive schedule), relative residual 1e-8.
 The timed form (default ``mixed_learned``) is the mixed-precision solver (FP32 V-cycle
-inside the FP64 CG) started from the learned initial guess (network on the 64x32x32 pooled
-cell grid; its inference is inside the timed solve).  One step = one complete solve
+inside the FP64 CG) with the learned coarse space: the network's predicted field (64x32x32
+pooled cell grid) spans a deflation space that gives the initial guess (the energy-optimal
+combination of its three components) and the coarse-grid correction of every PCG
+iteration; its inference is inside the timed solve.  One step = one complete solve
 including the hierarchy setup (the densities change every SIMP iteration, so the hierarchy
 is rebuilt every solve, as in the reference).  The plain FP64 MGCG and the other forms are
 timed beside it (``forms``), with their compliance and displacement errors against FP64,
 and the SIMP loops of the 192x96x96 (BF16 densities, 20 iterations) and 256x128x128
-(learned guess, 30 iterations) configurations report per-iteration errors against FP64.
+(learned coarse space, 30 iterations) configurations report per-iteration errors against
+FP64.
 
 Arms
   default          this library on N GPUs (one process per GPU, replicas: a solve does not
@@ -139,17 +142,17 @@ class Clocks:
 _NET = None
 
 
-def warm_start_for(learned, with_previous=False):
+def coarse_space_for(learned):
     global _NET
     if not learned:
         return None
     from pyfantom_b200 import learned as L
     if _NET is None:
         _NET = L.WarmStartNet.load()
-    return L.LearnedWarmStart(_NET, pool=4, read_stats=False, with_previous=with_previous)
+    return L.LearnedCoarseSpace(_NET, pool=4)
 
 
-def build_problem(nel, n_level, form="fp64", tol=1e-8, with_previous=False):
+def build_problem(nel, n_level, form="fp64", tol=1e-8):
     import torch
     from pyfantom_b200 import workloads
     from pyfantom_b200.CUDA import FiniteElement, MultiGrid, StructuredMesh3D, StructuredStiffnessKernel
@@ -159,7 +162,7 @@ def build_problem(nel, n_level, form="fp64", tol=1e-8, with_previous=False):
     mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
     kern = StructuredStiffnessKernel(mesh)
     sol = MultiGrid(mesh, kern, maxiter=1000, tol=tol, n_smooth=2, omega=0.6, n_level=n_level, precision=prec,
-                    warm_start=warm_start_for(learned, with_previous))
+                    coarse_correction=coarse_space_for(learned))
     fe = FiniteElement(mesh, kern, sol)
     fe.add_dirichlet_boundary_condition(node_ids=torch.as_tensor(wl["fixed_nodes"], device="cuda"), rhs=0.0)
     fe.add_point_forces(forces=wl["load_forces"], node_ids=torch.as_tensor(wl["load_nodes"], device="cuda"))
@@ -242,7 +245,7 @@ def run_ours(args, rank, world, local_rank):
         e0.record(stream)
         fe.rhs.copy_(rhs_h, non_blocking=True)
         E_dev.copy_(E_h, non_blocking=True)
-        fe.solver.last_x0 = None  # every timed solve starts cold (x0 = 0, or the learned guess)
+        fe.solver.last_x0 = None  # every timed solve starts cold (x0 = 0, or the learned space's guess)
         U2, _ = fe.solve(E_dev)
         U_h.copy_(U2, non_blocking=True)
         e1.record(stream)
@@ -290,7 +293,8 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded smoothed-random densities, cantilever loads)",
         "config": {"workload": args.workload, "form": args.form, "nel": list(nel), "dof": D, "n_level": nl,
                    "n_smooth": 2, "omega": 0.6, "tol": 1e-8,
-                   "start": "learned guess (network on nel/4 cells)" if FORMS[args.form][1] else "cold (x0 = 0)",
+                   "start": ("learned coarse space (network on nel/4 cells): deflated start and coarse-grid correction"
+                             if FORMS[args.form][1] else "cold (x0 = 0)"),
                    "l2": "512 MB L2 flush before every timed solve; inputs exceed L2",
                    "parallelism": f"replicas x{world}",
                    "warmup_extra": "untimed solves until 1 s has passed, so the clocks settle"},
@@ -352,7 +356,7 @@ def forms_at(workload, names=("fp64", "mixed", "mixed_bf16", "mixed_learned")):
             o["speedup_vs_fp64"] = round(out["fp64"]["ms"] / o["ms"], 3)
         out[name] = o
     if "mixed_learned" in out:
-        out["mixed_learned"]["guess"] = "network on nel/4 cells, energy-scaled"
+        out["mixed_learned"]["learned"] = "network on nel/4 cells as a deflation space (start + correction)"
     return out
 
 
@@ -407,8 +411,8 @@ def matvec_probe(workload, reps=8, warm=2):
 
 def simp_loop(workload, form, n_iter, vf=0.3, r_min=2.0, move=0.2):
     """SIMP minimum compliance with OC on the workload, the displacement solves by `form`
-    (the learned form offers the network's guess and the previous solution, whichever has
-    the lower energy).  Each iteration's stiffness is also solved by the plain FP64 MGCG
+    (the learned form starts from the previous solution corrected inside the network's
+    deflation space, and keeps that space as its coarse-grid correction).  Each iteration's stiffness is also solved by the plain FP64 MGCG
     (warm-started from its own previous solution, same tolerance) to give the relative
     compliance and displacement errors of the form; the time per SIMP iteration (filter,
     penalisation, solve, sensitivity, adjoint filter, OC update) excludes those checks."""
@@ -416,7 +420,7 @@ def simp_loop(workload, form, n_iter, vf=0.3, r_min=2.0, move=0.2):
     from pyfantom_b200.CUDA import MinimumCompliance, MultiGrid, OC, StructuredFilter3D
     spec = WORKLOADS[workload]
     nel, nl = spec["nel"], spec["n_level"]
-    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, form, with_previous=True)
+    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, form)
     ref = MultiGrid(mesh, kern, maxiter=1000, tol=1e-8, n_smooth=2, omega=0.6, n_level=nl, precision="fp64")
     prob = MinimumCompliance(fe, StructuredFilter3D(mesh, r_min), E_mul=[1.0], void=1e-9, penalty=3.0,
                              volume_fraction=[vf], heavyside=False)
