@@ -412,8 +412,9 @@ def matvec_probe(workload, reps=8, warm=2):
 def simp_loop(workload, form, n_iter, vf=0.3, r_min=2.0, move=0.2):
     """SIMP minimum compliance with OC on the workload, the displacement solves by `form`
     (the learned form starts from the previous solution corrected inside the network's
-    deflation space, and keeps that space as its coarse-grid correction).  Each iteration's stiffness is also solved by the plain FP64 MGCG
-    (warm-started from its own previous solution, same tolerance) to give the relative
+    deflation space, and keeps that space as its coarse-grid correction).  Each iteration's
+    stiffness is also solved by the plain FP64 MGCG (warm-started from its own previous
+    solution, same tolerance) to give the relative
     compliance and displacement errors of the form; the time per SIMP iteration (filter,
     penalisation, solve, sensitivity, adjoint filter, OC update) excludes those checks."""
     import torch
@@ -479,6 +480,48 @@ def probe_matvec(args):
     """Time the fine-level matvec alone (for ncu captures)."""
     return {"probe": "matvec", "workload": args.workload, **matvec_probe(args.workload, reps=args.steps,
                                                                            warm=args.warmup)}
+
+
+def probe_level1(args):
+    """The level-1 operator of the V-cycle alone in the form's precision, element-level and
+    assembled stencil (STORE epilogue, L2 flushed before every launch): microseconds and
+    algorithmic bytes (u and y once, the 8 Ehat per coarse element or the 126-value half
+    stencil per coarse node, one flag byte per coarse node)."""
+    import torch
+    from pyfantom_b200.CUDA import MultiGrid
+    spec = WORKLOADS[args.workload]
+    nel, nl = spec["nel"], spec["n_level"]
+    prec = FORMS[args.form][0]
+    wl, mesh, kern, sol, fe, E = build_problem(nel, nl, "fp64")
+    kern.set_rho(E)
+    flush = _flush_buffer()
+    dt, sz = (torch.float64, 8) if prec == "fp64" else (torch.float32, 4)
+    cnel = [n // 2 for n in nel]
+    Nn1, Ne1 = int(np.prod([n + 1 for n in cnel])), int(np.prod(cnel))
+    hbm, kind = peaks()
+    out = {"probe": "level1", "workload": args.workload, "precision": prec}
+    for op in ("element", "stencil"):
+        s = MultiGrid(mesh, kern, maxiter=10, tol=1e-8, n_smooth=2, omega=0.6, n_level=nl, precision=prec,
+                      coarse_op=op)
+        s.setup()
+        u = torch.randn(3 * Nn1, dtype=dt, device="cuda")
+        ts = []
+        for i in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            s.level_matvec(1, u)
+            e1.record()
+            e1.synchronize()
+            if i >= args.warmup:
+                ts.append(e0.elapsed_time(e1))
+        ms = statistics.median(ts)
+        byts = 2 * 3 * Nn1 * sz + (8 * Ne1 * sz + Nn1 if op == "element" else 126 * Nn1 * sz)
+        out[op] = {"us": round(ms * 1e3, 1), "algorithmic_bytes": byts, "GB_per_s": round(byts / ms / 1e6, 1),
+                   "frac_of_hbm": round(byts / ms / 1e6 / hbm, 4), "dirty": s.level_info()[1]}
+        del s
+    out["peak"] = {"GB_per_s": hbm, "kind": kind}
+    return out
 
 
 def probe_solve(args):
@@ -563,8 +606,8 @@ def main():
     ap.add_argument("--no-simp", action="store_true", help="skip the SIMP loops in the extras")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=3, help="PCG iterations of the CPU-baseline sample")
-    ap.add_argument("--probe", choices=["matvec", "solve"], default=None,
-                    help="only time the fine matvec or bracket one solve (for ncu captures)")
+    ap.add_argument("--probe", choices=["matvec", "level1", "solve"], default=None,
+                    help="only time the fine matvec, the level-1 operator, or bracket one solve (for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" and not args.probe else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -583,6 +626,9 @@ def main():
         return
     if args.probe == "solve":
         print(json.dumps(probe_solve(args)), flush=True)
+        return
+    if args.probe == "level1":
+        print(json.dumps(probe_level1(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -353,9 +353,8 @@ int pf_pgd_project_f64(long long n, const double* xs, const double* dg, double v
  * (16.9 MB held by every GPU that loads the library until the process exits).  Larger n
  * is rejected with PF_BAD_ARG.  The first call on each device resolves the array's
  * address with that device current and keeps it (it may also load the library's device
- * code), so that first call should come before any stream capture; after a
- * cudaDeviceReset the kept address is stale and the entry point must not be called
- * again in that process.  A non-NULL h_out makes the call wait for the stream to deliver
+ * code); after a cudaDeviceReset the kept address is stale and the entry point must not
+ * be called again in that process.  A non-NULL h_out makes the call wait for the stream to deliver
  * {||x_new - x||, lambda, steps}; pass NULL where the caller must not wait.  Calls share
  * the array: calls that overlap on the GPU race. */
 #define PF_OC_NOALLOC_MAX_ELEMS 2097152

@@ -72,7 +72,7 @@ struct pf_mg {
     // coarse-grid correction): field, W = A Q (FP32) and G^-1 (FP64, 9 values + 3 flags)
     int defl = 0;
     float* yf = nullptr;
-    float* Wf = nullptr;
+    double* Wd = nullptr;
     double* dG = nullptr;
     float* Ef = nullptr;            // FP32 element scales of the V-cycle (precision 1)
     __nv_bfloat16* Eb = nullptr;    // BF16 element scales of the V-cycle (precision 2)
@@ -331,9 +331,10 @@ __global__ void k_defl_comp(long long n, int dof, const float* __restrict__ yf, 
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = (int)(i % dof) == c ? (double)yf[i] : 0.0;
 }
-// partials of G_cd = q_c . W_d (9 per block, index c*3 + d, stride gridDim.x)
+// partials of G_cd = q_c . W_d (9 per block, index c*3 + d, stride gridDim.x); Q is the
+// FP32 field itself (an exact basis), W = K Q in FP64
 __global__ void __launch_bounds__(kRedThreads) k_defl_gram(long long n, int dof, const float* __restrict__ yf,
-                                                           const float* __restrict__ Wf, double* partials) {
+                                                           const double* __restrict__ Wd, double* partials) {
     __shared__ double s_red[kRedThreads / 32];
     double g[9];
 #pragma unroll
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(kRedThreads) k_defl_gram(long long n, int dof,
         const double y = yf[i];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const double t = y * (double)Wf[d * n + i];
+            const double t = y * Wd[d * n + i];
 #pragma unroll
             for (int cc = 0; cc < 3; cc++)
                 if (cc == c) g[cc * 3 + d] += t;
@@ -446,7 +447,7 @@ __global__ void k_defl_xadd(long long n, int dof, const float* __restrict__ yf, 
 // partials of r.z (index 0) and t_d = W_d . z (indices 1..3)
 template <typename TZ>
 __global__ void __launch_bounds__(kRedThreads) k_dot_defl(long long n, const double* __restrict__ r,
-                                                          const TZ* __restrict__ z, const float* __restrict__ Wf,
+                                                          const TZ* __restrict__ z, const double* __restrict__ Wd,
                                                           double* partials, const int* skip) {
     pdl_wait();
     pdl_trigger();
@@ -456,9 +457,9 @@ __global__ void __launch_bounds__(kRedThreads) k_dot_defl(long long n, const dou
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double zi = (double)z[i];
         a[0] += r[i] * zi;
-        a[1] += (double)Wf[i] * zi;
-        a[2] += (double)Wf[n + i] * zi;
-        a[3] += (double)Wf[2 * n + i] * zi;
+        a[1] += Wd[i] * zi;
+        a[2] += Wd[n + i] * zi;
+        a[3] += Wd[2 * n + i] * zi;
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -624,7 +625,7 @@ static void mg_free(pf_mg* mg) {
     coarse_destroy(mg->c1);
     mg->c1 = nullptr;
     for (void* p : {(void*)mg->K0_dev, (void*)mg->Kc_dev, (void*)mg->elem_flag, (void*)mg->node_flag, (void*)mg->Ef,
-                    (void*)mg->Eb, (void*)mg->yf, (void*)mg->Wf, (void*)mg->dG,
+                    (void*)mg->Eb, (void*)mg->yf, (void*)mg->Wd, (void*)mg->dG,
                     (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st,
                     (void*)mg->Eint, (void*)mg->bi, (void*)mg->xi})
         if (p) cudaFree(p);
@@ -911,7 +912,7 @@ static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaSt
         pf::count_launch();
         if (mg->defl)  // r.z and W^T z
             PF_CUDA(launch_pdl(k_dot_defl<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)mg->r,
-                               (const float*)res, (const float*)mg->Wf, mg->partials, (const int*)&mg->st->done));
+                               (const float*)res, (const double*)mg->Wd, mg->partials, (const int*)&mg->st->done));
         else
             PF_CUDA(launch_pdl(k_dot_partial<float>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, mg->r, res, mg->partials, &mg->st->done));
         PF_LAUNCH_CHECK("dot launch");
@@ -923,7 +924,7 @@ static int precondition(pf_mg* mg, const void** z_out, long long* np_out, cudaSt
             if ((s = vcycle<double>(mg, 0, mg->r, &res, nullptr, nullptr, st))) return s;
             pf::count_launch();
             PF_CUDA(launch_pdl(k_dot_defl<double>, dim3(vec_blocks(n)), dim3(kRedThreads), 0, st, n, (const double*)mg->r,
-                               (const double*)res, (const float*)mg->Wf, mg->partials, (const int*)&mg->st->done));
+                               (const double*)res, (const double*)mg->Wd, mg->partials, (const int*)&mg->st->done));
             PF_LAUNCH_CHECK("dot launch");
             *np_out = vec_blocks(n);
         } else {
@@ -1247,7 +1248,7 @@ extern "C" int pf_mg_set_deflation(pf_mg* mg, const double* y, void* stream) {
     int s = PF_OK;
     if (!mg->yf) {
         s = dalloc((void**)&mg->yf, (size_t)n * sizeof(float));
-        s = s ? s : dalloc((void**)&mg->Wf, (size_t)3 * n * sizeof(float));
+        s = s ? s : dalloc((void**)&mg->Wd, (size_t)3 * n * sizeof(double));
         s = s ? s : dalloc((void**)&mg->dG, 16 * sizeof(double));
         if (s) return s;
     }
@@ -1256,17 +1257,20 @@ extern "C" int pf_mg_set_deflation(pf_mg* mg, const double* y, void* stream) {
     const int dof = mg->op->grid.dof;
     k_defl_field<<<vb, kRedThreads, 0, st>>>(n, dof, y, mg->mask, mg->yf);
     PF_LAUNCH_CHECK("deflation field launch");
-    if (dof == 2) PF_CUDA(cudaMemsetAsync(mg->Wf + 2 * n, 0, (size_t)n * sizeof(float), st));
-    for (int c = 0; c < dof; c++) {  // W_c = A q_c, through the FP64 fine matvec (q, p as scratch)
+    if (dof == 2) PF_CUDA(cudaMemsetAsync(mg->Wd + 2 * n, 0, (size_t)n * sizeof(double), st));
+    // W_c = A q_c through the FP64 fine matvec (q as scratch), kept in FP64: with W rounded to
+    // FP32 the projection leaves Q^T r a drift of the rounding error every iteration, nothing
+    // in the deflated iteration removes it, and the solve diverges
+    for (int c = 0; c < dof; c++) {
         pf::count_launch();
         k_defl_comp<<<vb, kRedThreads, 0, st>>>(n, dof, mg->yf, c, mg->q);
         PF_LAUNCH_CHECK("deflation column launch");
-        Epi<double> e = make_epi<double>(PF_EPI_STORE, nullptr, nullptr, nullptr, nullptr, mg->p, nullptr, 1.0, nullptr);
+        Epi<double> e = make_epi<double>(PF_EPI_STORE, nullptr, nullptr, nullptr, nullptr, mg->Wd + (size_t)c * n,
+                                         nullptr, 1.0, nullptr);
         if ((s = launch_fine_matvec<double, double>(mg->op, mg->E, mg->q, mg->mask, e, st))) return s;
-        if ((s = launch_d2f(n, mg->p, mg->Wf + (size_t)c * n, st))) return s;
     }
     pf::count_launch(2);
-    k_defl_gram<<<vb, kRedThreads, 0, st>>>(n, dof, mg->yf, mg->Wf, mg->partials);
+    k_defl_gram<<<vb, kRedThreads, 0, st>>>(n, dof, mg->yf, (const double*)mg->Wd, mg->partials);
     k_defl_ginv<<<1, kRedThreads, 0, st>>>(mg->partials, (long long)vb, mg->dG);
     PF_LAUNCH_CHECK("deflation Gram launch");
     if (!mg->defl) drop_graphs(mg);  // the captured iterations are the plain ones

@@ -11,10 +11,10 @@
 // elements (16.9 MB); every GPU that loads this library holds it until the process exits.
 // Host code cannot use the array's name as a device address, so the first call on each
 // device resolves it with cudaGetSymbolAddress while that device is current and keeps
-// the pointer.  That first call may also load the library's device code, so it should
-// come before any stream capture.  A cudaDeviceReset invalidates the kept pointer: the
-// entry point must not be called again in that process.  All calls share the array and
-// it keeps the contents of the last call; the kernels initialise every value they read
+// the pointer; that first call may also load the library's device code.  A
+// cudaDeviceReset invalidates the kept pointer: the entry point must not be called again
+// in that process.  All calls share the array and it keeps the contents of the last
+// call; the kernels initialise every value they read
 // (the bisection state and all partial sums are written before use), so nothing needs
 // clearing between calls.  With a non-NULL h_out the call copies the result scalars to
 // the host and waits for the stream.  Calls that overlap on the GPU (different streams

@@ -6,7 +6,8 @@ DOFs); the solver starts from x0 = x + Q G^-1 Q^T (b - K x) and keeps its search
 K-orthogonal to Q.  Parity bar: the FP64 form takes the oracle's iteration count (+-1) and
 both reach the plain solve's solution (1e-8 relative, max-norm); the FP32 V-cycle form
 (precision 'mixed') reaches the same solution within +-2 iterations of the oracle.  The
-library keeps Q and K Q in FP32 (G is summed in FP64), the oracle in FP64.
+library rounds the field to FP32 (the basis Q) and keeps K Q in FP64; the oracle keeps both
+in FP64.
 """
 import numpy as np
 import pytest
