@@ -800,7 +800,7 @@ static void h8p_launch_dims(const Grid& g, dim3* grid, int* CXc) {
     *CXc = best;
     *grid = dim3(tz, ty, (nx + best - 1) / best);
 }
-static bool use_paired(const Op* op) { return op->grid.dim == 3 && op->cube && op->variant == 0; }
+static bool use_paired(const Op* op) { return op->grid.dim == 3 && op->cube && op->variant == 1; }
 
 // ---------------------------------------------------------------------------------------
 // 2D matvec (node gather, dense 8x8 K0)

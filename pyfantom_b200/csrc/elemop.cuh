@@ -29,7 +29,7 @@ struct pf_op {
     double coef[33];
     int sparse, cube;
     double cube_v[7];
-    int variant;  // FP32 fine matvec of cube elements: 0 two elements per lane (packed), 1 one
+    int variant;  // FP32 fine matvec of cube elements: 0 one element per lane, 1 two (packed)
 };
 
 namespace pf {

@@ -418,9 +418,9 @@ def test_guess_select_picks_lower_energy(lib):
                                  (13, 22, 186), (40, 12, 60)])
 @pytest.mark.parametrize("variant", [0, 1])
 def test_matvec_fp32_variants_tile_edges(lib, nel, variant):
-    """Both FP32 fine matvecs of cube elements (variant 0: two elements per thread in packed
-    FP32, 62 owned node columns per warp and 11 owned node rows per block; variant 1: one
-    element per thread) on grids around their tile edges (nz + 1 = 62, 63, 64, 125, 126,
+    """Both FP32 fine matvecs of cube elements (variant 0: one element per thread; variant 1:
+    two elements per thread in packed FP32, 62 owned node columns per warp and 11 owned node
+    rows per block) on grids around their tile edges (nz + 1 = 62, 63, 64, 125, 126,
     187), with constraints on a tenth of the DOFs, against the oracle, and bitwise
     repeatable."""
     rng = np.random.default_rng(sum(nel) + 17 * variant)
