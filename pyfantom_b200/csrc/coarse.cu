@@ -151,41 +151,68 @@ int coarse_factorise(const Op* op, double* coef /* [150] */) {
 // ---------------------------------------------------------------------------------------
 // setup: dirty-element list, Ehat, dirty Walsh matrices
 // ---------------------------------------------------------------------------------------
-constexpr int kScanThreads = 1024;
+constexpr int kScanThreads = 1024;  // flags per block of the compaction
 
-// dmap[e] = index of coarse element e in the dirty list (or -1), dlist[d] = e (d < cap),
-// *count = number of dirty elements; one block, elements in order
-__global__ void __launch_bounds__(kScanThreads) k_dirty_scan(long long ne, const uint8_t* __restrict__ elem_flag,
-                                                             int* __restrict__ dmap, int* __restrict__ dlist, int cap,
-                                                             int* __restrict__ count) {
-    __shared__ int s_cnt[kScanThreads];
-    const int t = threadIdx.x;
-    const long long lo = ne * t / kScanThreads, hi = ne * (t + 1) / kScanThreads;
-    int c = 0;
-    for (long long e = lo; e < hi; e++) c += elem_flag[e] ? 1 : 0;
-    s_cnt[t] = c;
-    __syncthreads();
-    // inclusive scan (Hillis-Steele)
-    for (int o = 1; o < kScanThreads; o <<= 1) {
-        const int v = t >= o ? s_cnt[t - o] : 0;
-        __syncthreads();
-        s_cnt[t] += v;
-        __syncthreads();
-    }
-    int d = s_cnt[t] - c;
-    for (long long e = lo; e < hi; e++) {
-        if (elem_flag[e]) {
-            dmap[e] = d;
-            if (d < cap) dlist[d] = (int)e;
-            d++;
-        } else {
-            dmap[e] = -1;
-        }
-    }
-    if (t == kScanThreads - 1) *count = s_cnt[t];
+// Stream compaction of a flag array in index order, in two passes: block b counts the
+// flags of items [1024 b, 1024 (b + 1)); then every block adds the counts of the blocks
+// before it and places its items with a ballot scan.  map[i] = rank of item i among the
+// flagged items (or -1), list[rank] = i (rank < cap), *count = number of flagged items.
+__global__ void __launch_bounds__(kScanThreads) k_flag_count(long long n, const uint8_t* __restrict__ flag,
+                                                             int* __restrict__ bcount) {
+    const long long i = (long long)blockIdx.x * kScanThreads + threadIdx.x;
+    const int c = __syncthreads_count(i < n && flag[i]);
+    if (threadIdx.x == 0) bcount[blockIdx.x] = c;
 }
 
-// Ehat of every coarse element in structure-of-arrays form Eh[k * ne + e]
+__global__ void __launch_bounds__(kScanThreads) k_flag_compact(long long n, const uint8_t* __restrict__ flag,
+                                                               const int* __restrict__ bcount, int* __restrict__ map,
+                                                               int* __restrict__ list, int cap, int* __restrict__ count) {
+    __shared__ int s_w[kScanThreads / 32];
+    __shared__ int s_base;
+    const int t = threadIdx.x, w = t >> 5, l = t & 31;
+    // base: the flagged items of all earlier blocks
+    int acc = 0;
+    for (int b = t; b < (int)blockIdx.x; b += kScanThreads) acc += bcount[b];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (l == 0) s_w[w] = acc;
+    __syncthreads();
+    if (t == 0) {
+        int sum = 0;
+        for (int q = 0; q < kScanThreads / 32; q++) sum += s_w[q];
+        s_base = sum;
+    }
+    __syncthreads();
+    const long long i = (long long)blockIdx.x * kScanThreads + t;
+    const bool f = i < n && flag[i];
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    s_w[w] = __popc(m);  // s_w is free again after the barrier above
+    __syncthreads();
+    int before = 0;
+    for (int q = 0; q < w; q++) before += s_w[q];
+    const int r = s_base + before + __popc(m & ((1u << l) - 1u));
+    if (i < n) {
+        map[i] = f ? r : -1;
+        if (f && r < cap) list[r] = (int)i;
+    }
+    if (blockIdx.x == gridDim.x - 1 && t == kScanThreads - 1) {
+        int tot = 0;
+        for (int q = 0; q < kScanThreads / 32; q++) tot += s_w[q];
+        *count = s_base + tot;
+    }
+}
+
+static int flag_compact(long long n, const uint8_t* flag, int* bcount, int* map, int* list, int cap, int* count,
+                        cudaStream_t st) {
+    const unsigned nb = (unsigned)((n + kScanThreads - 1) / kScanThreads);
+    pf::count_launch(2);
+    k_flag_count<<<nb, kScanThreads, 0, st>>>(n, flag, bcount);
+    k_flag_compact<<<nb, kScanThreads, 0, st>>>(n, flag, bcount, map, list, cap, count);
+    PF_LAUNCH_CHECK("flag compaction launch");
+    return PF_OK;
+}
+
+// Ehat of every coarse element, element-major Eh[e * 8 + k] (one 32-byte (FP32) or 64-byte
+// (FP64) run per element, read with vector loads)
 template <typename T>
 __global__ void k_coarse_ehat(int NXc, int NYc, int NZc, const double* __restrict__ E, const int* __restrict__ dmap,
                               T* __restrict__ Eh) {
@@ -213,7 +240,7 @@ __global__ void k_coarse_ehat(int NXc, int NYc, int NZc, const double* __restric
     const int d = dmap ? dmap[e] : -1;
     if (d >= 0) c[0] = -(double)d - 1.0;
 #pragma unroll
-    for (int q = 0; q < 8; q++) Eh[q * ne + e] = (T)c[q];
+    for (int q = 0; q < 8; q++) Eh[e * 8 + q] = (T)c[q];
 }
 
 template <int DIM>
@@ -426,7 +453,25 @@ __device__ __forceinline__ void coarse_element(const T (&glo)[3][2][2], const T 
             dirty = dlist[d] == e;
         }
     }
-    // outputs slot by slot (component a, y-mode, z-mode; x-modes 0 and 1), folded into G
+    // outputs slot by slot (component a, y-mode, z-mode; x-modes 0 and 1), folded into G.
+    // FP32: one branch per element between the explicit and the structured matrix; FP64
+    // (254 registers) branches per output, which keeps it free of spills
+    if (sizeof(T) == 4 && dirty) {
+        const T* wd = Wd + d;
+        Unroll<12>::run([&](auto S) {
+            constexpr int slot = decltype(S)::value;
+            constexpr int a = slot / 4, ym = (slot >> 1) & 1, zm = slot & 1;
+            constexpr int i0 = (((ym << 1) | (zm << 2)) * 3) + a, i1 = ((1 | (ym << 1) | (zm << 2)) * 3) + a;
+            T z0 = T(0), z1 = T(0);
+#pragma unroll
+            for (int j = 0; j < 24; j++) z0 = fma(wd[(long long)(i0 * 24 + j) * cap], v[j], z0);
+#pragma unroll
+            for (int j = 0; j < 24; j++) z1 = fma(wd[(long long)(i1 * 24 + j) * cap], v[j], z1);
+            G[a][ym][zm] = (z0 - z1) + carry[a][ym][zm];
+            carry[a][ym][zm] = z0 + z1;
+        });
+        return;
+    }
     Unroll<12>::run([&](auto S) {
         constexpr int slot = decltype(S)::value;
         constexpr int a = slot / 4, ym = (slot >> 1) & 1, zm = slot & 1;
@@ -435,26 +480,24 @@ __device__ __forceinline__ void coarse_element(const T (&glo)[3][2][2], const T 
             constexpr int xm = decltype(X)::value;
             constexpr int i = ((xm | (ym << 1) | (zm << 2)) * 3) + a;
             T acc = T(0);
-            if (dirty) {
+            if (sizeof(T) == 8 && dirty) {
                 const T* w = Wd + (long long)(i * 24) * cap + d;
 #pragma unroll
                 for (int j = 0; j < 24; j++) acc = fma(w[(long long)j * cap], v[j], acc);
-            } else {
-                if constexpr (i >= 3) {
-                    Unroll<8>::run([&](auto K) {
-                        constexpr int k = decltype(K)::value;
-                        constexpr int q = wclass(i) ^ k;
-                        constexpr int j0 = wslot(q, 0), j1 = wslot(q, 1), j2 = wslot(q, 2);
-                        constexpr int c0 = coarse_pat(i, j0), c1 = coarse_pat(i, j1), c2 = coarse_pat(i, j2);
-                        if constexpr (c0 >= 0 || c1 >= 0 || c2 >= 0) {
-                            T t = T(0);
-                            if constexpr (c0 >= 0) t = fma(cf.b[c0 < 0 ? 0 : c0], v[j0], t);
-                            if constexpr (c1 >= 0) t = fma(cf.b[c1 < 0 ? 0 : c1], v[j1], t);
-                            if constexpr (c2 >= 0) t = fma(cf.b[c2 < 0 ? 0 : c2], v[j2], t);
-                            acc = fma(eh[k], t, acc);
-                        }
-                    });
-                }
+            } else if constexpr (i >= 3) {
+                Unroll<8>::run([&](auto K) {
+                    constexpr int k = decltype(K)::value;
+                    constexpr int q = wclass(i) ^ k;
+                    constexpr int j0 = wslot(q, 0), j1 = wslot(q, 1), j2 = wslot(q, 2);
+                    constexpr int c0 = coarse_pat(i, j0), c1 = coarse_pat(i, j1), c2 = coarse_pat(i, j2);
+                    if constexpr (c0 >= 0 || c1 >= 0 || c2 >= 0) {
+                        T t = T(0);
+                        if constexpr (c0 >= 0) t = fma(cf.b[c0 < 0 ? 0 : c0], v[j0], t);
+                        if constexpr (c1 >= 0) t = fma(cf.b[c1 < 0 ? 0 : c1], v[j1], t);
+                        if constexpr (c2 >= 0) t = fma(cf.b[c2 < 0 ? 0 : c2], v[j2], t);
+                        acc = fma(eh[k], t, acc);
+                    }
+                });
             }
             zx[xm] = acc;
         });
@@ -507,7 +550,6 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     const int n1 = n0 + rows;
     const int eplane = NY * NZ;
     const int e0 = je * NZ + kc;
-    const int ne = NX * NY * NZ;
     // D = diag(1/tw): per-axis factors of this lane's node column and the two node rows
     const T sz = inv_tw<T>(kc, nz), sy0 = inv_tw<T>(je, ny), sy1 = inv_tw<T>(je + 1, ny);
     const T s0 = sz * sy0, s1 = sz * sy1;
@@ -546,9 +588,25 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     };
     auto eload = [&](int ie, T (&eh)[8]) {
         const bool ok = elem_ok && ie >= 0 && ie < NX;
-        const int e = e0 + eplane * ie;
+        const long long e = (long long)e0 + (long long)eplane * ie;
+        if (ok) {
+            if constexpr (sizeof(T) == 4) {
+                const float4* p = reinterpret_cast<const float4*>(Eh + e * 8);
+                const float4 a = p[0], b = p[1];
+                eh[0] = a.x, eh[1] = a.y, eh[2] = a.z, eh[3] = a.w;
+                eh[4] = b.x, eh[5] = b.y, eh[6] = b.z, eh[7] = b.w;
+            } else {
+                const double2* p = reinterpret_cast<const double2*>(Eh + e * 8);
 #pragma unroll
-        for (int k = 0; k < 8; k++) eh[k] = ok ? Eh[(long long)k * ne + e] : T(0);
+                for (int k = 0; k < 4; k++) {
+                    const double2 a = p[k];
+                    eh[2 * k] = a.x, eh[2 * k + 1] = a.y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) eh[k] = T(0);
+        }
     };
 
     T carry[3][2][2];
@@ -713,6 +771,10 @@ int coarse_create(const Op* op, int fp32, CoarseOp** out) {
     s = s ? s : calloc_dev((void**)&c->dmap, (size_t)ne * sizeof(int));
     s = s ? s : calloc_dev((void**)&c->nmap, (size_t)c->g.n_nodes * sizeof(int));
     s = s ? s : calloc_dev((void**)&c->count, 2 * sizeof(int));
+    {
+        const long long nmax = ne > c->g.n_nodes ? ne : c->g.n_nodes;
+        s = s ? s : calloc_dev((void**)&c->bcount, (size_t)((nmax + kScanThreads - 1) / kScanThreads) * sizeof(int));
+    }
     if (!s && cudaMallocHost((void**)&c->h_count, 2 * sizeof(int)) != cudaSuccess) s = fail(PF_NO_MEMORY, "pinned alloc");
     if (s) {
         coarse_destroy(c);
@@ -725,7 +787,7 @@ int coarse_create(const Op* op, int fp32, CoarseOp** out) {
 void coarse_destroy(CoarseOp* c) {
     if (!c) return;
     for (void* p : {c->Eh, (void*)c->dmap, (void*)c->dlist, (void*)c->M, c->Wd, (void*)c->count, (void*)c->nmap,
-                    (void*)c->nlist, c->S})
+                    (void*)c->nlist, c->S, (void*)c->bcount})
         if (p) cudaFree(p);
     if (c->h_count) cudaFreeHost(c->h_count);
     delete c;
@@ -753,10 +815,9 @@ int coarse_setup(CoarseOp* c, const double* E, const uint8_t* mask, const uint8_
     c->nflag = node_flag;
     if (mask) {
         for (int pass = 0; pass < 2; pass++) {
-            pf::count_launch(2);
-            k_dirty_scan<<<1, kScanThreads, 0, st>>>(ne, elem_flag, c->dmap, c->dlist, c->cap, c->count);
-            k_dirty_scan<<<1, kScanThreads, 0, st>>>(gc.n_nodes, node_flag, c->nmap, c->nlist, c->icap, c->count + 1);
-            PF_LAUNCH_CHECK("dirty scan launch");
+            int s = flag_compact(ne, elem_flag, c->bcount, c->dmap, c->dlist, c->cap, c->count, st);
+            s = s ? s : flag_compact(gc.n_nodes, node_flag, c->bcount, c->nmap, c->nlist, c->icap, c->count + 1, st);
+            if (s) return s;
             PF_CUDA(cudaMemcpyAsync(c->h_count, c->count, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
             PF_CUDA(cudaStreamSynchronize(st));
             nd = c->h_count[0];

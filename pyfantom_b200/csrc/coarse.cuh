@@ -17,6 +17,7 @@ struct CoarseOp {
     void* Wd = nullptr;           // dirty matrices, Walsh basis [576][cap], V-cycle precision
     int* count = nullptr;         // device: number of dirty elements, number of identity nodes
     int* h_count = nullptr;       // pinned copy
+    int* bcount = nullptr;        // per-block counts of the flag compactions
     int cap = 0, ndirty = 0;
     // identity rows R (I - Z) P of the constrained fine DOFs, applied per coarse node in the
     // physical basis (kept out of the Walsh-basis dirty matrices, where their O(1) entries
