@@ -439,7 +439,8 @@ def simp_loop(workload, form, n_iter, vf=0.3, r_min=2.0, move=0.2):
         c = float(prob.f())
         row.update(compliance=c, rel_compliance_err=abs(c - cr) / abs(cr),
                    rel_displacement_err=float(torch.linalg.norm(U - Ur) / torch.linalg.norm(Ur)),
-                   pcg_iterations=sol.last_info["iterations"], fp64_pcg_iterations=ref.last_info["iterations"])
+                   pcg_iterations=sol.last_info["iterations"], fp64_pcg_iterations=ref.last_info["iterations"],
+                   status=sol.last_info["status"], fp64_status=ref.last_info["status"])
         rows.append(row)
 
     check({"iteration": 0})
@@ -452,11 +453,15 @@ def simp_loop(workload, form, n_iter, vf=0.3, r_min=2.0, move=0.2):
         t_iter.append(e0.elapsed_time(e1))
         its.append(sol.last_info["iterations"])
         check({"iteration": it + 1, "ms": round(t_iter[-1], 2)})
+    ok = [r for r in rows if r["fp64_status"] == "PF_OK"] or rows
     out = {"workload": workload, "form": form, "iterations": n_iter, "volfrac": vf, "r_min": r_min,
            "ms_per_simp_iteration": round(statistics.mean(t_iter), 2),
            "mean_pcg_iterations": round(statistics.mean(its), 2),
-           "max_rel_compliance_err": max(r["rel_compliance_err"] for r in rows),
-           "max_rel_displacement_err": max(r["rel_displacement_err"] for r in rows),
+           "max_rel_compliance_err": max(r["rel_compliance_err"] for r in ok),
+           "max_rel_displacement_err": max(r["rel_displacement_err"] for r in ok),
+           "errors_over": "iterations where the FP64 check solve converged",
+           "iterations_fp64_not_converged": [r["iteration"] for r in rows if r["fp64_status"] != "PF_OK"],
+           "iterations_form_not_converged": [r["iteration"] for r in rows if r["status"] != "PF_OK"],
            "per_iteration": [{k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in r.items()}
                              for r in rows]}
     del wl, mesh, kern, sol, fe, E, ref, prob, oc
