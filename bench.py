@@ -175,6 +175,22 @@ def _flush_buffer():
     return torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
 
+def replica_max(ms, world, device):
+    """Max over ranks of one rank's device time: replicas run independent solves and the job
+    ends with the slowest rank (no data-path collective; this all-reduce is timing only)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, steps, max_ms):
+    """Whole-job solves/s: every rank solved `steps` times within the slowest rank's time."""
+    return round(world * steps / (max_ms / 1e3), 4)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -227,10 +243,7 @@ def run_ours(args, rank, world, local_rank):
     launches = lib.pf_launch_count() - launches0
     if world > 1:
         dist.barrier()
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = replica_max(total_ms, world, "cuda")
     clk = clocks.stop() if rank == 0 else None
 
     # ---- end to end through the public API with host buffers --------------------------
@@ -251,10 +264,7 @@ def run_ours(args, rank, world, local_rank):
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_max = float(te.item())
+    e2e_max = replica_max(e2e_ms, world, "cuda")
 
     # ---- roofline of the dominant kernel: the fine-level matvec of the V-cycle (FP32 in
     # the mixed forms, FP64 in the FP64 form), every launch of one solve timed live with
@@ -286,7 +296,7 @@ def run_ours(args, rank, world, local_rank):
     dtype = {"fp64": "f64", "mixed": "f64 outer / f32 V-cycle", "mixed_bf16": "f64 outer / f32 V-cycle / bf16 E",
              "mixed_learned": "f64 outer / f32 V-cycle"}[args.form]
     result = {
-        "metric": METRIC, "value": round(world * args.steps / (max_ms / 1e3), 4), "unit": "solves/s",
+        "metric": METRIC, "value": replica_throughput(world, args.steps, max_ms), "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": dtype,
@@ -299,7 +309,7 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}",
                    "warmup_extra": "untimed solves until 1 s has passed, so the clocks settle"},
         "pcg_iterations": iters, "status": status, "compliance": compliance,
-        "e2e": {"value": round(world * args.steps / (e2e_max / 1e3), 4), "unit": "solves/s",
+        "e2e": {"value": replica_throughput(world, args.steps, e2e_max), "unit": "solves/s",
                 "h2d_bytes_per_step": int(8 * (D + Ne)), "d2h_bytes_per_step": int(8 * D)},
         "gpu_launches": int(launches),
         "roofline": roof,
