@@ -95,9 +95,9 @@ def install() -> None:
         for k, v in attrs.items():
             setattr(m, k, v)
         mods[name] = m
-    for name, m in mods.items():  # parent.child attributes
-        parent, _, child = name.rpartition(".")
-        if parent in mods:
+    for name, m in mods.items():  # parent.child attributes; a class of the same name wins, as
+        parent, _, child = name.rpartition(".")  # after the reference's `from .X import *`
+        if parent in mods and child not in table[parent]:
             setattr(mods[parent], child, m)
 
 

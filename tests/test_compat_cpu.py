@@ -20,6 +20,10 @@ def test_reference_import_paths_resolve_to_the_library():
         assert StructuredMesh3D is geom.CuStructuredMesh3D and StructuredMesh2D is geom.CuStructuredMesh2D
         assert CuStructuredFilter3D is geom.CuStructuredFilter3D
         assert OC2 is OC
+        from pyfantom_b200.FiniteElement import FiniteElement as FE
+        from pyfantom_b200.Problem import MinimumCompliance as MC
+        from pyFANTOM.FiniteElement.CUDA.FiniteElement import FiniteElement as FE2
+        assert FiniteElement is FE is FE2 and MinimumCompliance is MC
         compat.install()  # idempotent
         with pytest.raises(ImportError):
             from pyFANTOM.CUDA import GeneralStiffnessKernel  # noqa: F401  (not on the structured path)
