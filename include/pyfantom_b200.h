@@ -69,6 +69,14 @@ int pf_op_destroy(pf_op* op);
 int pf_op_set_variant(pf_op* op, int variant);
 /* node mask from a per-DOF bool array (pyFANTOM/stiffness/CUDA/_FEA.py:441-456) */
 int pf_pack_mask(const pf_op* op, const uint8_t* con_dof, uint8_t* node_mask, void* stream);
+/* Explicit CSR of the matrix the matvec applies, Z K(E) Z + (I - Z) (StructuredStiffnessKernel.
+ * construct, pyFANTOM/stiffness/CUDA/_FEA.py:484-516): row_ptr [n_dof + 1], col and val
+ * [pf_csr_nnz(op)], int32 indices, columns increasing within a row; the pattern depends on
+ * the grid only (couplings of constrained DOFs are stored as zeros).  PF_UNSUPPORTED when
+ * the nonzeros exceed 32-bit indices. */
+long long pf_csr_nnz(const pf_op* op);
+int pf_construct_csr_f64(const pf_op* op, const double* E, const uint8_t* node_mask, int* row_ptr, int* col,
+                         double* val, void* stream);
 
 /* y = K(E) u with Dirichlet identity rows: y_c = u_c at constrained DOFs, constrained
  * columns skipped.  Replaces mat_vec_node_basis_parallel[_wcon]_cuda_kernel

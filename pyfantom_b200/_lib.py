@@ -72,6 +72,8 @@ SIGNATURES = {
     "pf_op_destroy": (_I, [_P]),
     "pf_op_set_variant": (_I, [_P, _I]),
     "pf_pack_mask": (_I, [_P, _P, _P, _P]),
+    "pf_csr_nnz": (_LL, [_P]),
+    "pf_construct_csr_f64": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "pf_matvec_f64": (_I, [_P, _P, _P, _P, _P, _P]),
     "pf_matvec_f32": (_I, [_P, _P, _P, _P, _P, _P]),
     "pf_matvec_f32_bf16": (_I, [_P, _P, _P, _P, _P, _P]),

@@ -10,6 +10,9 @@
 #include "mgkern.cuh"
 
 namespace pf {
+long long csr_nnz(const Grid& g);
+int launch_construct_csr(const Grid& g, const double* E, const uint8_t* mask, const double* K0_dev, int* row_ptr,
+                         int* col, double* val, cudaStream_t st);
 
 static thread_local char g_err[1024] = "";
 static std::atomic<unsigned long long> g_launches{0};
@@ -137,6 +140,14 @@ extern "C" int pf_op_destroy(pf_op* op) {
         if (p) cudaFree(p);
     delete h;
     return PF_OK;
+}
+
+extern "C" long long pf_csr_nnz(const pf_op* op) { return op ? pf::csr_nnz(op->grid) : -1; }
+
+extern "C" int pf_construct_csr_f64(const pf_op* op, const double* E, const uint8_t* node_mask, int* row_ptr, int* col,
+                                    double* val, void* stream) {
+    if (!op || !E || !row_ptr || !col || !val) return fail(PF_BAD_ARG, "pf_construct_csr_f64: NULL argument");
+    return launch_construct_csr(op->grid, E, node_mask, holder(op)->aux.K0, row_ptr, col, val, as_stream(stream));
 }
 
 extern "C" int pf_pack_mask(const pf_op* op, const uint8_t* con_dof, uint8_t* node_mask, void* stream) {

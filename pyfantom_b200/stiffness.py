@@ -75,6 +75,7 @@ class StructuredStiffnessKernel(StiffnessKernel):
         self.idx_map = torch.arange(n, dtype=torch.int32, device=device())
         self.non_con_map = self.idx_map
         self.has_been_constructed = False
+        self._csr_vals = None
         self.ptr = None
         self._grid = _lib.make_grid(self.nel)
         handle = ctypes.c_void_p()
@@ -193,13 +194,30 @@ class StructuredStiffnessKernel(StiffnessKernel):
         return self.dk
 
     def construct(self, rho):
-        raise NotImplementedError("explicit CSR assembly (construct) is not part of this library; "
-                                  "use CG or MultiGrid")
+        """Explicit sparse matrix on the GPU (reference _FEA.py:484-516): a torch CSR tensor
+        (int32 indices, float64 values) of the matrix ``dot`` applies, Z K(rho) Z + (I - Z)
+        with Z zeroing the constrained DOFs.  The sparsity pattern is kept across calls
+        (``self.ptr``), as the reference keeps its ``indptr``."""
+        L = _lib.load()
+        rho = as_cuda(rho, torch.float64)
+        n = self.shape[0]
+        dev = device()
+        if not self.has_been_constructed or self._csr_vals is None:
+            nnz = int(L.pf_csr_nnz(self._op))
+            self.ptr = torch.empty(n + 1, dtype=torch.int32, device=dev)
+            self._csr_cols = torch.empty(nnz, dtype=torch.int32, device=dev)
+            self._csr_vals = torch.empty(nnz, dtype=torch.float64, device=dev)
+        _lib.check(L.pf_construct_csr_f64(self._op, _lib.ptr(rho), self._mask_ptr(), _lib.ptr(self.ptr),
+                                          _lib.ptr(self._csr_cols), _lib.ptr(self._csr_vals), _lib.stream()))
+        self.CSR = torch.sparse_csr_tensor(self.ptr, self._csr_cols, self._csr_vals, size=(n, n))
+        self.has_been_constructed = True
+        return self.CSR
 
     def reset(self):
         self.has_rho = False
         self.rho = None
         self.has_been_constructed = False
+        self._csr_vals = None
         self.constraints[:] = False
         self.node_mask.zero_()
         self.has_con = False
