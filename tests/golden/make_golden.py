@@ -407,6 +407,61 @@ def solve_goldens():
     save("solve16", **out)
 
 
+def odd_goldens():
+    """2D grids with odd element counts, where every coarse grid floors nel / 2
+    (core/CPU/_mgm.py, as core/CUDA/_mgm.py:24-27): restriction / prolongation, the Galerkin
+    levels 1 and 2 with Dirichlet rows, and a MultiGrid solve of an MBB beam whose 3 coarse
+    levels are 15x5 -> 7x2 -> 3x1 (at odd sizes the prolongation is not R^T, and the
+    reference's PCG stagnates near 1e-3; the solve is recorded as it comes out) and one
+    V-cycle on its hierarchy."""
+    rng = np.random.default_rng(2024)
+    out = {}
+    for tag, nel in [("a", (7, 5)), ("b", (9, 6)), ("c", (6, 3))]:
+        nel_a = np.array(nel, dtype=np.int32)
+        nf = int(np.prod(nel_a + 1))
+        nc = int(np.prod(nel_a // 2 + 1))
+        vf = rng.standard_normal(nf * 2)
+        vc = rng.standard_normal(nc * 2)
+        out[f"{tag}_nel"] = nel_a
+        out[f"{tag}_vf"] = vf
+        out[f"{tag}_vc"] = vc
+        out[f"{tag}_restricted"] = np.array(apply_restriction(vf, nel_a, 2))
+        out[f"{tag}_prolonged"] = np.array(apply_prolongation(vc, nel_a, 2))
+        mesh = StructuredMesh2D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
+        kern = StructuredStiffnessKernel(mesh)
+        E = rng.uniform(1e-3, 1.0, mesh.elements.shape[0])
+        kern.set_rho(E)
+        x0 = np.where(mesh.nodes[:, 0] == 0)[0]
+        cons = np.unique(np.concatenate([(x0[:, None] * 2 + np.arange(2)).reshape(-1),
+                                         rng.choice(mesh.nodes.shape[0] * 2, size=3, replace=False)]))
+        kern.add_constraints(cons)
+        A1 = get_restricted_l0(mesh, kern)
+        A2 = get_restricted_l1p(A1, mesh.nel // 2, 2)
+        out[f"{tag}_E"] = E
+        out[f"{tag}_cons"] = cons
+        out[f"{tag}_A1"] = A1.toarray()
+        out[f"{tag}_A2"] = A2.toarray()
+    wl = workloads.mbb2d(30, 10)
+    fac = lambda m, k: MultiGrid(m, k, maxiter=500, tol=1e-10, n_smooth=2, omega=0.6, n_level=3, cycle="V")  # noqa: E731
+    _, kern, fe, _ = _simp_setup(wl, fac, 1.5, 0.5)
+    U, res = fe.solve(wl["E"])
+    out["mbb_U"] = np.array(U)
+    out["mbb_res"] = np.array(res)
+    out["mbb_E"] = wl["E"]
+    # one V-cycle from a zero guess with level-0 Jacobi weight 0.45 (the reference's own
+    # _multi_grid on the hierarchy the solve built)
+    r = rng.standard_normal(np.array(fe.rhs).shape[0])
+    r[np.nonzero(kern.constraints)[0]] = 0.0
+    solver = fe.solver
+    solver.matrix_free = False
+    solver._setup()
+    solver.coarse_solve = solver._coarse_solver(solver.levels[-1][0])
+    solver.omega = 0.45
+    out["mbb_r"] = r
+    out["mbb_z"] = np.array(solver._multi_grid(np.zeros_like(r), r.copy(), 0))
+    save("odd2d", **out)
+
+
 def cg_goldens():
     """Textbook CG iterates: the reference's own CG loop (solvers/CPU/_solvers.py:111-139)
     run from x0 = 0 with rtol = 0 (never stops early), so that after maxiter = N it returns
@@ -460,6 +515,7 @@ def main():
     sensitivity_goldens()
     solve_goldens()
     cg_goldens()
+    odd_goldens()
     f = mbb_trajectory()
     pgd_goldens()
     multimaterial_goldens()

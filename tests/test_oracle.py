@@ -234,3 +234,34 @@ def test_oracle_deflated_pcg():
     y = np.random.default_rng(0).standard_normal(x.size)
     x2, it2, _, st2 = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=2, tol=1e-10, deflation=y)
     assert st2 == 0 and abs(it2 - it) <= 3 and rel(x2, x) < 1e-8
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_odd_2d_transfers_and_galerkin(golden, tag):
+    """2D grids with odd element counts (coarse grids floor nel / 2): restriction,
+    prolongation (where P differs from R^T: a fine node past the last coarse node takes
+    that node's value) and the Galerkin levels against the reference's own code."""
+    g = golden("odd2d")
+    nel = tuple(int(v) for v in g[tag + "_nel"])
+    assert np.array_equal(O.restrict(nel, g[tag + "_vf"]), g[tag + "_restricted"])
+    assert np.array_equal(O.prolong(nel, g[tag + "_vc"]), g[tag + "_prolonged"])
+    K0 = unit_K0(2)
+    A1 = O.galerkin_l0(nel, K0, g[tag + "_E"], g[tag + "_cons"])
+    D1 = O.stencil_to_dense(O.coarse_nel(nel), A1)
+    assert rel(D1, g[tag + "_A1"]) < 1e-13
+    A2 = O.galerkin_l1p(O.coarse_nel(nel), A1)
+    D2 = O.stencil_to_dense(O.coarse_nel(O.coarse_nel(nel)), A2)
+    assert rel(D2, g[tag + "_A2"]) < 1e-13
+
+
+def test_odd_2d_vcycle_matches_reference(golden):
+    """MBB 30x10 with 3 levels (15x5, 7x2, 3x1): one V-cycle from a zero guess on the
+    reference's own hierarchy (its _multi_grid) equals the oracle's.  At odd sizes the
+    prolongation is not R^T, so the V-cycle is not symmetric and the PCG stagnates: the
+    reference's solve stops at maxiter with a relative residual near 1e-3."""
+    g = golden("odd2d")
+    wl = workloads.mbb2d(30, 10)
+    z = O.mg_vcycle((30, 10), unit_K0(2), g["mbb_E"], wl["fixed_dofs"], g["mbb_r"], n_level=3, n_smooth=2,
+                    omega=0.45)
+    assert rel(z, g["mbb_z"]) < 1e-12
+    assert float(g["mbb_res"]) > 1e-4
