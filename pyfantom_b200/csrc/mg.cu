@@ -666,9 +666,10 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
     if (cfg->precision < 0 || cfg->precision > 2)
         return fail(PF_BAD_ARG, "precision must be 0 (fp64), 1 (fp32 V-cycle) or 2 (fp32 V-cycle, bf16 densities)");
     const Grid& g = op->grid;
+    // every level floors nel / 2 (core/CUDA/_mgm.py:24-27); the coarsest keeps an element per axis
     for (int a = 0; a < g.dim; a++)
-        if (g.nel[a] % (1 << cfg->n_level) != 0)
-            return fail(PF_BAD_ARG, "nel[%d]=%d is not divisible by 2^n_level=%d", a, g.nel[a], 1 << cfg->n_level);
+        if ((g.nel[a] >> cfg->n_level) < 1)
+            return fail(PF_BAD_ARG, "nel[%d]=%d has no element left after %d halvings", a, g.nel[a], cfg->n_level);
     pf_mg* mg = new pf_mg();
     mg->op = op;
     mg->cfg = *cfg;
@@ -681,8 +682,10 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
         delete mg;
         return fail(PF_BAD_ARG, "coarse_op must be 0 (element operator on level 1 when available) or 1 (stencils)");
     }
-    // level 1 element by element when it is smoothed (not the coarsest) and K0 allows it
-    if (cfg->coarse_op == 0 && g.dim == 3 && mg->nlev >= 2) {
+    // level 1 element by element when it is smoothed (not the coarsest), its coarse elements
+    // cover the fine grid (even element counts) and K0 allows it
+    const bool even = g.nel[0] % 2 == 0 && g.nel[1] % 2 == 0 && (g.dim == 2 || g.nel[2] % 2 == 0);
+    if (cfg->coarse_op == 0 && g.dim == 3 && mg->nlev >= 2 && even) {
         double coef[150];
         if (coarse_factorise(op, coef) == PF_OK) s = coarse_create(op, mg->fp32, &mg->c1);
         if (!s) set_error("");

@@ -123,7 +123,9 @@ __global__ void k_restrict(GridDev<DIM> gf, GridDev<DIM> gc, const TI* __restric
 }
 
 // One thread per fine node (all DIM components, contiguous loads of each parent): P =
-// Phat diag(1/tw), the mean of the 1, 2, 4 or 8 parent values divided by their tw.
+// Phat diag(1/tw), the mean of the 1, 2, 4 or 8 parent values divided by their tw.  With an
+// odd element count the last fine node along that axis has a single parent and takes its
+// value (mgm.cu:198-244 averages over the parents that exist), so there P is not R^T.
 template <int DIM, typename T>
 __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict__ vc, T* __restrict__ vf,
                           const int* skip) {
@@ -135,7 +137,9 @@ __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict_
     int i, j, k;
     ndec(gf, f, i, j, k);
     const int i0 = i >> 1, j0 = j >> 1, k0 = DIM == 3 ? k >> 1 : 0;
-    const int i1 = i0 + (i & 1), j1 = j0 + (j & 1), k1 = DIM == 3 ? k0 + (k & 1) : 0;
+    // an odd fine node past the last coarse node (odd element count) has one parent
+    const int i1 = min(i0 + (i & 1), gc.nn[0] - 1), j1 = min(j0 + (j & 1), gc.nn[1] - 1);
+    const int k1 = DIM == 3 ? min(k0 + (k & 1), gc.nn[2] - 1) : 0;
     auto itw = [&](int c, int n) { return (c == 0 || c == n - 1) ? T(1.0 / 1.5) : T(0.5); };
     T acc[DIM];
 #pragma unroll
@@ -152,8 +156,8 @@ __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict_
             }
         }
     }
-    const int nodd = (i & 1) + (j & 1) + (DIM == 3 ? (k & 1) : 0);
-    const T scale = nodd == 0 ? T(1) : nodd == 1 ? T(0.5) : nodd == 2 ? T(0.25) : T(0.125);
+    const int npar = (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1);  // the mean over the parents
+    const T scale = npar == 1 ? T(1) : npar == 2 ? T(0.5) : npar == 4 ? T(0.25) : T(0.125);
 #pragma unroll
     for (int d = 0; d < DIM; d++) vf[f * DIM + d] = acc[d] * scale;
 }
@@ -406,18 +410,26 @@ __global__ void __launch_bounds__(128) k_galerkin_l0(GridDev<DIM> gf, GridDev<DI
         // coarse elements containing I as local corner LI
         for (int LI = 0; LI < NC; LI++) {
             const int ex = ic - kCXd(LI), ey = jc - kCYd(LI), ez = DIM == 3 ? kc - kCZd(LI) : 0;
-            if (ex < 0 || ey < 0 || ex >= gc.nel[0] || ey >= gc.nel[1]) continue;
-            if (DIM == 3 && (ez < 0 || ez >= gc.nel[2])) continue;
+            // past the last coarse node of an axis with an odd element count lies a virtual
+            // coarse element: its far corners do not exist and only its near children do
+            const bool vx = ex == gc.nel[0] && gf.nel[0] > 2 * gc.nel[0];
+            const bool vy = ey == gc.nel[1] && gf.nel[1] > 2 * gc.nel[1];
+            const bool vz = DIM == 3 && ez == gc.nel[2] && gf.nel[2] > 2 * gc.nel[2];
+            if (ex < 0 || ey < 0 || (ex >= gc.nel[0] && !vx) || (ey >= gc.nel[1] && !vy)) continue;
+            if (DIM == 3 && (ez < 0 || (ez >= gc.nel[2] && !vz))) continue;
             // J must be a corner of the same element
             const int lx = kCXd(LI) + ox, ly = kCYd(LI) + oy, lz = DIM == 3 ? kCZd(LI) + oz : 0;
             if (lx < 0 || lx > 1 || ly < 0 || ly > 1 || lz < 0 || lz > 1) continue;
+            if ((vx && (kCXd(LI) || lx)) || (vy && (kCYd(LI) || ly)) || (vz && (kCZd(LI) || lz))) continue;
             int LJ = 0;
             for (int q = 0; q < NC; q++)
                 if (kCXd(q) == lx && kCYd(q) == ly && (DIM == 2 || kCZd(q) == lz)) LJ = q;
+            const bool virt = vx || vy || vz;
             const long long ce = DIM == 3 ? ((long long)ex * gc.nel[1] + ey) * gc.nel[2] + ez : (long long)ex * gc.nel[1] + ey;
-            const bool dirty = elem_flag[ce] != 0;
+            const bool dirty = virt || elem_flag[ce] != 0;  // virtual elements check their masks
             for (int c = 0; c < NC; c++) {
                 const int fx = 2 * ex + kCXd(c), fy = 2 * ey + kCYd(c), fz = DIM == 3 ? 2 * ez + kCZd(c) : 0;
+                if (fx >= gf.nel[0] || fy >= gf.nel[1] || (DIM == 3 && fz >= gf.nel[2])) continue;
                 const long long fe = DIM == 3 ? ((long long)fx * gf.nel[1] + fy) * gf.nel[2] + fz : (long long)fx * gf.nel[1] + fy;
                 const double we = E[fe];
                 if (!dirty) {
@@ -433,13 +445,13 @@ __global__ void __launch_bounds__(128) k_galerkin_l0(GridDev<DIM> gf, GridDev<DI
                         double pl = (1.0 - 0.5 * abs(nxl - 2 * kCXd(LI))) * (1.0 - 0.5 * abs(nyl - 2 * kCYd(LI)));
                         if (DIM == 3) pl *= 1.0 - 0.5 * abs(nzl - 2 * kCZd(LI));
                         if (pl == 0.0) continue;
-                        const uint8_t ml = mask[nidx(gf, 2 * ex + nxl, 2 * ey + nyl, 2 * ez + nzl)];
+                        const uint8_t ml = mask ? mask[nidx(gf, 2 * ex + nxl, 2 * ey + nyl, 2 * ez + nzl)] : 0;
                         for (int l2 = 0; l2 < NC; l2++) {
                             const int nx2 = kCXd(c) + kCXd(l2), ny2 = kCYd(c) + kCYd(l2), nz2 = DIM == 3 ? kCZd(c) + kCZd(l2) : 0;
                             double p2 = (1.0 - 0.5 * abs(nx2 - 2 * kCXd(LJ))) * (1.0 - 0.5 * abs(ny2 - 2 * kCYd(LJ)));
                             if (DIM == 3) p2 *= 1.0 - 0.5 * abs(nz2 - 2 * kCZd(LJ));
                             if (p2 == 0.0) continue;
-                            const uint8_t m2 = mask[nidx(gf, 2 * ex + nx2, 2 * ey + ny2, 2 * ez + nz2)];
+                            const uint8_t m2 = mask ? mask[nidx(gf, 2 * ex + nx2, 2 * ey + ny2, 2 * ez + nz2)] : 0;
                             const double f = we * pl * p2;
                             for (int a = 0; a < DIM; a++) {
                                 if (ml & (1 << a)) continue;

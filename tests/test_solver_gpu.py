@@ -172,9 +172,10 @@ def test_status_breakdown_on_zero_operator():
 
 
 def test_bad_level_count_is_rejected():
+    """Four halvings of 12x8x8 leave no element on the coarsest level."""
     from pyfantom_b200._lib import PFError
     wl = workloads.cantilever3d(12, 8, 8)
-    _, kern, sol, fe = setup_problem(wl, 3)
+    _, kern, sol, fe = setup_problem(wl, 4)
     with pytest.raises(PFError):
         fe.solve(torch.as_tensor(wl["E"], device="cuda"))
 
@@ -284,3 +285,45 @@ def test_simp_loop_mixed_forms_track_fp64(prec):
         cr = float(torch.dot(fe.rhs, Ur))
         assert abs(float(prob.f()) - cr) < 1e-6 * abs(cr)
         assert float(torch.linalg.norm(prob._U - Ur) / torch.linalg.norm(Ur)) < 1e-5
+
+
+@pytest.mark.parametrize("case", [("mbb", (30, 10), 3), ("mbb", (7, 5), 2), ("mbb", (9, 6), 2),
+                                  ("cant", (9, 6, 5), 2), ("cant", (12, 8, 8), 3)])
+def test_odd_element_counts_match_oracle(case):
+    """Grids whose element counts are odd on some level (every coarse grid floors nel / 2,
+    as the reference): level-1 operator, one V-cycle and the first PCG iterates against the
+    oracle.  At odd sizes the prolongation is not R^T and the reference's PCG stagnates, so
+    iterates are compared, not converged solutions."""
+    kind, nel, nl = case
+    wl = workloads.cantilever3d(*nel) if kind == "cant" else workloads.mbb2d(*nel)
+    K0 = unit_K0(len(nel))
+    mesh, kern, sol, fe = setup_problem(wl, nl, tol=1e-14, maxiter=3)
+    E = torch.as_tensor(wl["E"], device="cuda")
+    kern.set_rho(E)
+    sol.setup()
+    rng = np.random.default_rng(5)
+    cn = tuple(n // 2 for n in nel)
+    u = rng.standard_normal(int(np.prod(np.array(cn) + 1)) * len(nel))
+    A1 = O.galerkin_l0(nel, K0, wl["E"], wl["fixed_dofs"])
+    y = sol.level_matvec(1, torch.as_tensor(u, device="cuda")).cpu().numpy()
+    assert rel(y, O.stencil_matvec(cn, A1, u)) < 1e-12
+    r = rng.standard_normal(kern.shape[0])
+    r[wl["fixed_dofs"]] = 0.0
+    z = sol.vcycle(torch.as_tensor(r, device="cuda"), omega=0.45).cpu().numpy()
+    zr = O.mg_vcycle(nel, K0, wl["E"], wl["fixed_dofs"], r, n_level=nl, n_smooth=2, omega=0.45)
+    assert rel(z, zr) < 1e-10
+    U, res = sol.solve(fe.rhs, rho=E, use_last=False)
+    xo, ito, _, _ = O.mgcg_solve(nel, K0, wl["E"], wl["fixed_dofs"], wl["rhs"], n_level=nl, tol=1e-14, maxiter=3)
+    assert sol.last_info["iterations"] == ito == 3
+    assert rel(U.cpu().numpy(), xo) < 1e-9
+
+
+def test_odd_2d_vcycle_matches_reference_golden(golden):
+    """The reference's own V-cycle on the MBB 30x10 hierarchy (15x5, 7x2, 3x1)."""
+    g = golden("odd2d")
+    wl = workloads.mbb2d(30, 10)
+    mesh, kern, sol, fe = setup_problem(wl, 3)
+    kern.set_rho(torch.as_tensor(g["mbb_E"], device="cuda"))
+    sol.setup()
+    z = sol.vcycle(torch.as_tensor(g["mbb_r"], device="cuda"), omega=0.45).cpu().numpy()
+    assert rel(z, g["mbb_z"]) < 1e-10
