@@ -6,6 +6,9 @@
 // restriction R = diag(1/tw) Phat^T and prolongation P = Phat diag(1/tw) = R^T, where Phat
 // is trilinear (bilinear) interpolation (weights 0.5^{|d|_1} on the 3^DIM fine nodes
 // around an even fine node) and tw(c) = prod over axes of (1.5 on a boundary, else 2).
+// Coarse grids floor nel / 2; along an axis with an odd element count the last fine node
+// has one coarse parent, which the prolongation copies (there P differs from R^T, while
+// the Galerkin product uses R^T throughout, as the reference).
 // Coarse operators are Galerkin R A P with A_fine = Z K Z + I - Z on level 0
 // (mgm.cu:247-447) and R A_l P on deeper levels (mgm.cu:449-590).
 #include "common.cuh"
