@@ -285,6 +285,17 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_beta(const double* partials
     }
 }
 
+// component i % dof of a grid-stride loop, advanced without a 64-bit division per element
+struct CompIter {
+    int c, step, dof;
+    __device__ CompIter(long long i0, long long stride, int d)
+        : c((int)(i0 % d)), step((int)(stride % d)), dof(d) {}
+    __device__ __forceinline__ void next() {
+        c += step;
+        if (c >= dof) c -= dof;
+    }
+};
+
 // p = z + beta p (init: p = z); with the deflation field yf, z - Q coef in place of z
 template <typename TZ>
 __global__ void k_pcg_p(long long n, const TZ* __restrict__ z, double* __restrict__ p, const PcgState* st, int init,
@@ -294,13 +305,19 @@ __global__ void k_pcg_p(long long n, const TZ* __restrict__ z, double* __restric
     if (st->done) return;
     const double b = st->beta;
     const double c0 = st->coef[0], c1 = st->coef[1], c2 = st->coef[2];
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double zi = (double)z[i];
-        if (yf) {
-            const int c = (int)(i % dof);
-            zi -= (double)yf[i] * (c == 0 ? c0 : c == 1 ? c1 : c2);
+    const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    if (yf) {
+        CompIter ci(i0, stride, dof);
+#pragma unroll 4
+        for (long long i = i0; i < n; i += stride, ci.next()) {
+            const double zi = (double)z[i] - (double)yf[i] * (ci.c == 0 ? c0 : ci.c == 1 ? c1 : c2);
+            p[i] = init ? zi : zi + b * p[i];
         }
-        p[i] = init ? zi : zi + b * p[i];
+    } else {
+        for (long long i = i0; i < n; i += stride) {
+            const double zi = (double)z[i];
+            p[i] = init ? zi : zi + b * p[i];
+        }
     }
 }
 
@@ -454,6 +471,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dot_defl(long long n, const dou
     __shared__ double s_red[kRedThreads / 32];
     if (skip && *skip) return;
     double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double zi = (double)z[i];
         a[0] += r[i] * zi;
