@@ -684,13 +684,21 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 }
 
 // FP64: 8 warps, 1 block per SM (the operator holds 24 Walsh values and 8 Ehat in
-// registers); FP32: 8 warps, 2 blocks per SM
-constexpr int kCNW = 8;
+// registers); FP32: 8 warps, 2 blocks per SM (measured: 74.7 us per 256x128x128 level-1
+// launch against 81.9 us for one block of 16 warps, whose halo rows are fewer but whose
+// step barrier holds all 16 warps)
+template <typename T>
+struct CoarseShape {  // warps per block (NW - 1 owned element rows) and blocks per SM
+    static constexpr int NW = 8;
+    static constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
+};
 
-static void coarse_launch_dims(const Grid& g, bool fp32, dim3* grid, int* CXc) {
+template <typename T>
+static void coarse_launch_dims(const Grid& g, dim3* grid, int* CXc) {
+    constexpr int NW = CoarseShape<T>::NW;
     const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
-    const int tz = (nz + kCZTile - 1) / kCZTile, ty = (ny + kCNW - 2) / (kCNW - 1);
-    const long long slots = (long long)kNumSM * (fp32 ? 2 : 1);
+    const int tz = (nz + kCZTile - 1) / kCZTile, ty = (ny + NW - 2) / (NW - 1);
+    const long long slots = (long long)kNumSM * CoarseShape<T>::MINB;
     const long long cols = (long long)tz * ty;
     int best = 2;
     long long best_cost = -1;
@@ -709,9 +717,9 @@ static void coarse_launch_dims(const Grid& g, bool fp32, dim3* grid, int* CXc) {
 template <typename T, int MODE>
 static int coarse_launch(dim3 grid, int cx, const Grid& g, const T* u, const CoarseOp* c, const CoarseCoef<T>& cf,
                          const Epi<T>& epi, cudaStream_t st) {
-    constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
+    constexpr int NW = CoarseShape<T>::NW, MINB = CoarseShape<T>::MINB;
     const uint8_t* nflag = c->nident > 0 ? c->nflag : nullptr;
-    PF_CUDA(launch_pdl(k_coarse_matvec<T, kCNW, MINB, MODE>, grid, dim3(kCNW * 32), 0, st, g.nel[0], g.nel[1],
+    PF_CUDA(launch_pdl(k_coarse_matvec<T, NW, MINB, MODE>, grid, dim3(NW * 32), 0, st, g.nel[0], g.nel[1],
                        g.nel[2], cx, u, (const T*)c->Eh, (const T*)c->Wd, (const int*)c->dlist, c->cap, cf, epi,
                        nflag, (const int*)c->nmap, (const T*)c->S, c->icap));
     return PF_OK;
@@ -724,7 +732,7 @@ int launch_coarse_matvec(const CoarseOp* c, const Grid& g, const T* u, const Epi
     for (int q = 0; q < kCoarseCoefs; q++) cf.b[q] = (T)c->coef[q];
     dim3 grid;
     int cx;
-    coarse_launch_dims(g, sizeof(T) == 4, &grid, &cx);
+    coarse_launch_dims<T>(g, &grid, &cx);
     pf::count_launch();
     switch (epi.mode) {
         case PF_EPI_STORE:

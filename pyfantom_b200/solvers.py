@@ -190,6 +190,7 @@ class MultiGrid(Solver):
         self.coarse_op = coarse_op
         self._min_omega_arg = min_omega
         self._mg = None
+        self._side = None
         self.last_info = None
 
     def _ensure(self):
@@ -269,9 +270,19 @@ class MultiGrid(Solver):
             warm = True
         else:
             x = torch.empty(n, dtype=torch.float64, device=device())
-        self.setup()
+        y = None
         if self.coarse_correction is not None:
-            y = as_cuda(self.coarse_correction.field(k, rhs), torch.float64)
+            # the network runs on a side stream while the hierarchy is built on this one: it
+            # needs only rho, the load and the constraints
+            main = torch.cuda.current_stream()
+            if self._side is None:
+                self._side = torch.cuda.Stream()
+            self._side.wait_stream(main)
+            with torch.cuda.stream(self._side):
+                y = as_cuda(self.coarse_correction.field(k, rhs), torch.float64)
+        self.setup()
+        if y is not None:
+            main.wait_stream(self._side)
             _lib.check(_lib.load().pf_mg_set_deflation(self._mg, _lib.ptr(y), _lib.stream()))
         info = _lib.pf_solve_info()
         _lib.check(_lib.load().pf_mg_solve(self._mg, _lib.ptr(rhs), _lib.ptr(x), int(warm), float(self.tol),
