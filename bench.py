@@ -370,7 +370,7 @@ def forms_at(workload, names=("fp64", "mixed", "mixed_bf16", "mixed_learned")):
     return out
 
 
-def matvec_probe(workload, reps=8, warm=2):
+def matvec_probe(workload, reps=8, warm=2, fp32_variant=0):
     """The fine matvec alone (FP64, FP32, FP32 with BF16 element scales), L2 flushed before
     every launch: microseconds, algorithmic bytes and GB/s, DOF-matvecs/s."""
     import torch
@@ -381,6 +381,7 @@ def matvec_probe(workload, reps=8, warm=2):
     w = workloads.cantilever3d(*nel)
     mesh = StructuredMesh3D(*nel, *nel, physics=LinearElasticity(E=1.0, nu=0.3))
     kern = StructuredStiffnessKernel(mesh)
+    _lib.check(_lib.load().pf_op_set_variant(kern._op, int(fp32_variant)))
     kern.add_constraints(torch.as_tensor(w["fixed_dofs"], device="cuda"))
     D, Ne, Nn = kern.shape[0], int(np.prod(nel)), kern.n_nodes
     flush = _flush_buffer()
@@ -493,8 +494,8 @@ def extras(args):
 
 def probe_matvec(args):
     """Time the fine-level matvec alone (for ncu captures)."""
-    return {"probe": "matvec", "workload": args.workload, **matvec_probe(args.workload, reps=args.steps,
-                                                                           warm=args.warmup)}
+    return {"probe": "matvec", "workload": args.workload, "fp32_variant": args.fp32_variant,
+            **matvec_probe(args.workload, reps=args.steps, warm=args.warmup, fp32_variant=args.fp32_variant)}
 
 
 def probe_level1(args):
@@ -621,6 +622,8 @@ def main():
     ap.add_argument("--no-simp", action="store_true", help="skip the SIMP loops in the extras")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=3, help="PCG iterations of the CPU-baseline sample")
+    ap.add_argument("--fp32-variant", type=int, default=0, choices=[0, 1],
+                    help="FP32 fine matvec of cube elements in the matvec probe (pf_op_set_variant)")
     ap.add_argument("--probe", choices=["matvec", "level1", "solve"], default=None,
                     help="only time the fine matvec, the level-1 operator, or bracket one solve (for ncu captures)")
     args = ap.parse_args()
