@@ -165,12 +165,153 @@ __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict_
     for (int d = 0; d < DIM; d++) vf[f * DIM + d] = acc[d] * scale;
 }
 
+// 3D restriction by fine lines: block q = (ic, jc) stages the nine fine z-lines
+// (2ic + di, 2jc + dj), di, dj in {-1, 0, 1}, in shared memory with coalesced loads, then
+// each thread forms coarse nodes (ic, jc, kc) from them; same weights, normalisation and
+// fused first Jacobi sweep as k_restrict (which serves lines too long for shared memory).
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(128) k_restrict_lines(GridDev<3> gf, GridDev<3> gc, const TI* __restrict__ vf,
+                                                        TO* __restrict__ vc, const int* skip, Jacobi0<TO> j0) {
+    pdl_wait();
+    pdl_trigger();
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    TI* sl = reinterpret_cast<TI*>(s_raw);
+    using TA = TO;
+    if (skip && *skip) return;
+    const int q = blockIdx.x;
+    const int ic = q % gc.nn[0], jc = q / gc.nn[0];
+    const int L = 3 * gf.nn[2];
+    for (int line = 0; line < 9; line++) {
+        const int fi = 2 * ic + line % 3 - 1, fj = 2 * jc + line / 3 - 1;
+        const bool ok = fi >= 0 && fi < gf.nn[0] && fj >= 0 && fj < gf.nn[1];
+        const TI* src = ok ? vf + nidx(gf, fi, fj, 0) * 3 : nullptr;
+        for (int t = threadIdx.x; t < L; t += blockDim.x) sl[line * L + t] = ok ? src[t] : TI(0);
+    }
+    __syncthreads();
+    const TA ti = (ic == 0 || ic == gc.nn[0] - 1) ? TA(1.0 / 1.5) : TA(0.5);
+    const TA tj = (jc == 0 || jc == gc.nn[1] - 1) ? TA(1.0 / 1.5) : TA(0.5);
+    for (int kc = threadIdx.x; kc < gc.nn[2]; kc += blockDim.x) {
+        const TA tk = (kc == 0 || kc == gc.nn[2] - 1) ? TA(1.0 / 1.5) : TA(0.5);
+        const int fk = 2 * kc;
+        const bool lo = fk - 1 >= 0, hi = fk + 1 < gf.nn[2];
+        TA acc[3] = {TA(0), TA(0), TA(0)};
+#pragma unroll
+        for (int dj = -1; dj <= 1; dj++) {
+            TA accj[3] = {TA(0), TA(0), TA(0)};
+#pragma unroll
+            for (int di = -1; di <= 1; di++) {
+                const TI* r = sl + ((dj + 1) * 3 + (di + 1)) * L;
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    TA v = (TA)r[3 * fk + d];
+                    if (lo) v += TA(0.5) * (TA)r[3 * (fk - 1) + d];
+                    if (hi) v += TA(0.5) * (TA)r[3 * (fk + 1) + d];
+                    accj[d] += di == 0 ? v : TA(0.5) * v;
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) acc[d] += dj == 0 ? accj[d] : TA(0.5) * accj[d];
+        }
+        const long long c = nidx(gc, ic, jc, kc);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const TO bc = (TO)(acc[d] * ti * tj * tk);
+            vc[c * 3 + d] = bc;
+            if (j0.x) j0.x[c * 3 + d] = (TO)((*j0.omega) * j0.scale) * j0.dinv[c * 3 + d] * bc;
+        }
+    }
+}
+
+// 3D prolongation by cells: one thread per coarse node (ic, jc, kc) writes the up-to-8 fine
+// nodes (2ic + di, 2jc + dj, 2kc + dk), d in {0, 1}, from the up-to-8 coarse nodes
+// (ic + a, jc + b, kc + c).  Each coarse value is read once per thread instead of once per
+// fine child, and each thread writes two contiguous fine nodes (6 values) per (di, dj), so a
+// warp's stores of consecutive kc are contiguous.  Per axis a fine node at 2c takes parent c,
+// one at 2c + 1 the mean of c and c + 1, or c alone past the last coarse node (odd count):
+// the same values as k_prolong.
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_cells(GridDev<3> gf, GridDev<3> gc, const T* __restrict__ vc,
+                                                       T* __restrict__ vf, const int* skip) {
+    pdl_wait();
+    pdl_trigger();
+    if (skip && *skip) return;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= gc.n_nodes) return;
+    int ic, jc, kc;
+    ndec(gc, c, ic, jc, kc);
+    auto itw = [](int v, int n) { return (v == 0 || v == n - 1) ? T(1.0 / 1.5) : T(0.5); };
+    const bool hx = ic + 1 < gc.nn[0], hy = jc + 1 < gc.nn[1], hz = kc + 1 < gc.nn[2];  // upper parents
+    const bool fx = 2 * ic + 1 < gf.nn[0], fy = 2 * jc + 1 < gf.nn[1], fz = 2 * kc + 1 < gf.nn[2];  // odd children
+    // z stage for the four (a, b) parent columns: values at fine k = 2kc (z0) and 2kc + 1 (z1)
+    T z0[2][2][3], z1[2][2][3];
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            const bool ok = (a == 0 || hx) && (b == 0 || hy);
+            const int pi = ic + (ok ? a : 0), pj = jc + (ok ? b : 0);
+            const T wab = itw(pi, gc.nn[0]) * itw(pj, gc.nn[1]);
+            const T* v0 = vc + nidx(gc, pi, pj, kc) * 3;
+            const T w0 = wab * itw(kc, gc.nn[2]);
+            T lo[3], hi[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) lo[d] = ok ? w0 * v0[d] : T(0);
+            if (hz) {
+                const T* v1 = vc + nidx(gc, pi, pj, kc + 1) * 3;
+                const T w1 = wab * itw(kc + 1, gc.nn[2]);
+#pragma unroll
+                for (int d = 0; d < 3; d++) hi[d] = ok ? T(0.5) * (lo[d] + w1 * v1[d]) : T(0);
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; d++) hi[d] = lo[d];
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                z0[a][b][d] = lo[d];
+                z1[a][b][d] = hi[d];
+            }
+        }
+    // y then x stages, written per (di, dj) as the two z-neighbouring fine nodes
+#pragma unroll
+    for (int di = 0; di < 2; di++) {
+        if (di && !fx) continue;
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++) {
+            if (dj && !fy) continue;
+            T o0[3], o1[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                // along y for column a, then along x
+                T ya0[2], ya1[2];
+#pragma unroll
+                for (int a = 0; a < 2; a++) {
+                    ya0[a] = dj == 0 ? z0[a][0][d] : (hy ? T(0.5) * (z0[a][0][d] + z0[a][1][d]) : z0[a][0][d]);
+                    ya1[a] = dj == 0 ? z1[a][0][d] : (hy ? T(0.5) * (z1[a][0][d] + z1[a][1][d]) : z1[a][0][d]);
+                }
+                o0[d] = di == 0 ? ya0[0] : (hx ? T(0.5) * (ya0[0] + ya0[1]) : ya0[0]);
+                o1[d] = di == 0 ? ya1[0] : (hx ? T(0.5) * (ya1[0] + ya1[1]) : ya1[0]);
+            }
+            T* out = vf + nidx(gf, 2 * ic + di, 2 * jc + dj, 2 * kc) * 3;
+#pragma unroll
+            for (int d = 0; d < 3; d++) out[d] = o0[d];
+            if (fz) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) out[3 + d] = o1[d];
+            }
+        }
+    }
+}
+
 template <typename TI, typename TO>
 int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaStream_t st, Jacobi0<TO> j0) {
     const Grid gc = coarse_grid(gf);
     const unsigned nb = (unsigned)((gc.n_nodes * gf.dim + 255) / 256);
     pf::count_launch();
-    if (gf.dim == 3)
+    const size_t lines_bytes = (size_t)9 * 3 * gf.nn[2] * sizeof(TI);
+    if (gf.dim == 3 && lines_bytes <= 48 * 1024)
+        PF_CUDA(launch_pdl(k_restrict_lines<TI, TO>, dim3((unsigned)(gc.nn[0] * gc.nn[1])), dim3(128), lines_bytes, st,
+                           gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0));
+    else if (gf.dim == 3)
         PF_CUDA(launch_pdl(k_restrict<3, TI, TO>, dim3(nb), dim3(256), 0, st, gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0));
     else
         PF_CUDA(launch_pdl(k_restrict<2, TI, TO>, dim3(nb), dim3(256), 0, st, gdev<2>(gf), gdev<2>(gc), vf, vc, skip, j0));
@@ -183,7 +324,8 @@ int launch_prolong(const Grid& gf, const T* vc, T* vf, const int* skip, cudaStre
     const unsigned nb = (unsigned)((gf.n_nodes + 255) / 256);
     pf::count_launch();
     if (gf.dim == 3)
-        PF_CUDA(launch_pdl(k_prolong<3, T>, dim3(nb), dim3(256), 0, st, gdev<3>(gf), gdev<3>(gc), vc, vf, skip));
+        PF_CUDA(launch_pdl(k_prolong_cells<T>, dim3((unsigned)((gc.n_nodes + 255) / 256)), dim3(256), 0, st,
+                           gdev<3>(gf), gdev<3>(gc), vc, vf, skip));
     else
         PF_CUDA(launch_pdl(k_prolong<2, T>, dim3(nb), dim3(256), 0, st, gdev<2>(gf), gdev<2>(gc), vc, vf, skip));
     PF_LAUNCH_CHECK("prolong launch");

@@ -14,7 +14,9 @@
   ``warm_start`` (an object with ``guess(kernel, rhs)``, e.g. learned.LearnedWarmStart,
   that supplies the initial guess of a solve that does not reuse ``last_x0``) and
   ``coarse_op`` ('element': level 1 applied element by element from the fine densities
-  when the element allows it, the default; 'stencil': assembled stencils on every level)
+  when the element allows it; 'stencil': assembled stencils on every level; 'auto', the
+  default: element by element in the FP32 V-cycle of the mixed forms, where it is faster
+  than the FP32 stencil, and the stencil in the FP64 form, where the stencil is faster)
   and ``coarse_correction`` (an object with ``field(kernel, rhs)``, e.g.
   learned.LearnedCoarseSpace, whose nodal field spans a deflation space of the PCG,
   ``pf_mg_set_deflation``).
@@ -149,7 +151,7 @@ class MultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="cholmod", matrix_free=False, low_level_tol=1e-8,
                  low_level_maxiter=5000, min_omega=0.4, omega_boost=1.06, *, precision="fp64", check_every=4,
-                 warm_start=None, coarse_op="element", coarse_correction=None):
+                 warm_start=None, coarse_op="auto", coarse_correction=None):
         self.kernel = kernel
         self.warm_start = warm_start
         self.coarse_correction = coarse_correction
@@ -185,8 +187,8 @@ class MultiGrid(Solver):
             raise NotImplementedError("the lower-case 'w' (W-cycle) branch is not implemented; use 'V' or 'W'")
         if precision not in ("fp64", "mixed", "mixed_bf16"):
             raise ValueError("precision must be 'fp64', 'mixed' or 'mixed_bf16'")
-        if coarse_op not in ("element", "stencil"):
-            raise ValueError("coarse_op must be 'element' or 'stencil'")
+        if coarse_op not in ("auto", "element", "stencil"):
+            raise ValueError("coarse_op must be 'auto', 'element' or 'stencil'")
         self.coarse_op = coarse_op
         self._min_omega_arg = min_omega
         self._mg = None
@@ -205,7 +207,8 @@ class MultiGrid(Solver):
         cfg.coarse_beta = 1e-6
         cfg.precision = {"fp64": 0, "mixed": 1, "mixed_bf16": 2}[self.precision]
         cfg.check_every = int(self.check_every)
-        cfg.coarse_op = 0 if self.coarse_op == "element" else 1
+        element = self.coarse_op == "element" or (self.coarse_op == "auto" and self.precision != "fp64")
+        cfg.coarse_op = 0 if element else 1
         h = ctypes.c_void_p()
         _lib.check(_lib.load().pf_mg_create(self.kernel._op, ctypes.byref(cfg), ctypes.byref(h)))
         self._mg = h

@@ -119,7 +119,7 @@ def test_level1_repeated_setup_and_growing_dirty_set():
     kern = StructuredStiffnessKernel(mesh)
     wl = workloads.cantilever3d(*nel)
     kern.add_constraints(torch.as_tensor(wl["fixed_dofs"], device="cuda"))
-    sol = MultiGrid(mesh, kern, maxiter=300, tol=1e-10, n_smooth=2, omega=0.6, n_level=2)
+    sol = MultiGrid(mesh, kern, maxiter=300, tol=1e-10, n_smooth=2, omega=0.6, n_level=2, coarse_op="element")
     rhs = torch.as_tensor(wl["rhs"], device="cuda")
     cons = np.array(wl["fixed_dofs"])
     for step in range(4):
@@ -130,6 +130,7 @@ def test_level1_repeated_setup_and_growing_dirty_set():
             kern.add_constraints(torch.as_tensor(extra, device="cuda"))
         U, res = sol.solve(rhs, rho=torch.as_tensor(E, device="cuda"), use_last=False)
         assert sol.last_info["status"] == "PF_OK" and res < 1e-10
+        assert sol.level_info()[0]
         u = rng.standard_normal(int(np.prod(np.array(nel) // 2 + 1)) * 3)
         y = sol.level_matvec(1, torch.as_tensor(u, device="cuda")).cpu().numpy()
         A1 = O.galerkin_l0(nel, unit_K0(3), E, cons)

@@ -232,6 +232,26 @@ def test_transfers_golden(lib, golden, tag):
     assert rel(N(of), g[tag + "_prolonged"]) < 1e-15
 
 
+@pytest.mark.parametrize("nel", [(5, 4, 3), (7, 6, 9), (8, 4, 6), (2, 3, 2), (9, 5), (6, 7)])
+def test_transfers_odd_and_even_sizes(lib, nel):
+    """Restriction and prolongation (the 3D one by 2x2x2 cells of fine nodes) on grids with
+    odd element counts, where the last fine node of an odd axis has a single parent, against
+    the oracle (pinned to the reference on odd 2D grids)."""
+    rng = np.random.default_rng(sum(nel))
+    grid = lib.make_grid(nel)
+    dim = len(nel)
+    vf = rng.standard_normal(O.n_nodes(nel) * dim)
+    vc = rng.standard_normal(O.n_nodes(O.coarse_nel(nel)) * dim)
+    oc = torch.empty(vc.size, dtype=torch.float64, device="cuda")
+    of = torch.empty(vf.size, dtype=torch.float64, device="cuda")
+    vft, vct = T(vf), T(vc)
+    L = lib.load()
+    lib.check(L.pf_restrict_f64(ctypes.byref(grid), lib.ptr(vft), lib.ptr(oc), lib.stream()))
+    lib.check(L.pf_prolong_f64(ctypes.byref(grid), lib.ptr(vct), lib.ptr(of), lib.stream()))
+    assert rel(N(oc), O.restrict(nel, vf)) < 1e-15
+    assert rel(N(of), O.prolong(nel, vc)) < 1e-15
+
+
 def _soa_to_blocks(A, nn, dim):
     nb = 27 if dim == 3 else 9
     return A.reshape(nb, dim, dim, nn).transpose(3, 0, 1, 2)
