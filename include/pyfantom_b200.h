@@ -100,7 +100,8 @@ int pf_sensitivity_f64(const pf_op* op, const double* U, double* dk, void* strea
 
 /* ---- grid transfers (restriction_3d/2d_kernel, prolongation_3d/2d_kernel,
  *      pyFANTOM/core/CUDA/Kernels/mgm.cu:1-244, via core/CUDA/_mgm.py:173-264) ---------- */
-/* `fine` is the fine grid; the coarse grid has nel/2 elements (nel must be even). */
+/* `fine` is the fine grid (at least 2 elements per axis); the coarse grid has floor(nel/2)
+ * elements per axis, as the reference's (core/CUDA/_mgm.py:24-27). */
 int pf_restrict_f64(const pf_grid* fine, const double* vf, double* vc, void* stream);
 int pf_prolong_f64(const pf_grid* fine, const double* vc, double* vf, void* stream);
 

@@ -218,17 +218,19 @@ extern "C" int pf_adjoint_f64(const pf_op* op, const double* U, const double* rh
     return launch_adjoint(op, U, rho, *p, scale, out, as_stream(stream));
 }
 
-static int even_grid(const pf_grid* fine, Grid* g) {
+// a fine grid with a coarse level: at least two elements per axis (the coarse grid floors
+// nel / 2, core/CUDA/_mgm.py:24-27)
+static int coarsenable_grid(const pf_grid* fine, Grid* g) {
     int s = validate_grid(fine, g);
     if (s) return s;
     for (int a = 0; a < g->dim; a++)
-        if (g->nel[a] % 2) return fail(PF_BAD_ARG, "fine grid nel[%d]=%d must be even", a, g->nel[a]);
+        if (g->nel[a] < 2) return fail(PF_BAD_ARG, "fine grid nel[%d]=%d has no coarse level", a, g->nel[a]);
     return PF_OK;
 }
 
 extern "C" int pf_restrict_f64(const pf_grid* fine, const double* vf, double* vc, void* stream) {
     Grid g;
-    int s = even_grid(fine, &g);
+    int s = coarsenable_grid(fine, &g);
     if (s) return s;
     if (!vf || !vc) return fail(PF_BAD_ARG, "pf_restrict_f64: NULL argument");
     return launch_restrict<double, double>(g, vf, vc, nullptr, as_stream(stream));
@@ -236,7 +238,7 @@ extern "C" int pf_restrict_f64(const pf_grid* fine, const double* vf, double* vc
 
 extern "C" int pf_prolong_f64(const pf_grid* fine, const double* vc, double* vf, void* stream) {
     Grid g;
-    int s = even_grid(fine, &g);
+    int s = coarsenable_grid(fine, &g);
     if (s) return s;
     if (!vf || !vc) return fail(PF_BAD_ARG, "pf_prolong_f64: NULL argument");
     return launch_prolong<double>(g, vc, vf, nullptr, as_stream(stream));
@@ -253,7 +255,7 @@ extern "C" int pf_galerkin_l0_f64(const pf_op* op, const double* E, const uint8_
     if (!op || !E || !A_coarse) return fail(PF_BAD_ARG, "pf_galerkin_l0_f64: NULL argument");
     const Grid& g = op->grid;
     for (int a = 0; a < g.dim; a++)
-        if (g.nel[a] % 2) return fail(PF_BAD_ARG, "fine grid nel[%d]=%d must be even", a, g.nel[a]);
+        if (g.nel[a] < 2) return fail(PF_BAD_ARG, "fine grid nel[%d]=%d has no coarse level", a, g.nel[a]);
     pf_op_holder* h = holder(op);
     cudaStream_t st = as_stream(stream);
     const Grid g1 = coarse_grid(g);
@@ -269,7 +271,7 @@ extern "C" int pf_galerkin_l0_f64(const pf_op* op, const double* E, const uint8_
 
 extern "C" int pf_galerkin_l1p_f64(const pf_grid* fine, const double* A_fine, double* A_coarse, void* stream) {
     Grid g;
-    int s = even_grid(fine, &g);
+    int s = coarsenable_grid(fine, &g);
     if (s) return s;
     if (!A_fine || !A_coarse) return fail(PF_BAD_ARG, "pf_galerkin_l1p_f64: NULL argument");
     return launch_galerkin_l1p(g, A_fine, A_coarse, as_stream(stream));

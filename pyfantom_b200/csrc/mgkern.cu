@@ -165,63 +165,6 @@ __global__ void k_prolong(GridDev<DIM> gf, GridDev<DIM> gc, const T* __restrict_
     for (int d = 0; d < DIM; d++) vf[f * DIM + d] = acc[d] * scale;
 }
 
-// 3D restriction by fine lines: block q = (ic, jc) stages the nine fine z-lines
-// (2ic + di, 2jc + dj), di, dj in {-1, 0, 1}, in shared memory with coalesced loads, then
-// each thread forms coarse nodes (ic, jc, kc) from them; same weights, normalisation and
-// fused first Jacobi sweep as k_restrict (which serves lines too long for shared memory).
-template <typename TI, typename TO>
-__global__ void __launch_bounds__(128) k_restrict_lines(GridDev<3> gf, GridDev<3> gc, const TI* __restrict__ vf,
-                                                        TO* __restrict__ vc, const int* skip, Jacobi0<TO> j0) {
-    pdl_wait();
-    pdl_trigger();
-    extern __shared__ __align__(16) unsigned char s_raw[];
-    TI* sl = reinterpret_cast<TI*>(s_raw);
-    using TA = TO;
-    if (skip && *skip) return;
-    const int q = blockIdx.x;
-    const int ic = q % gc.nn[0], jc = q / gc.nn[0];
-    const int L = 3 * gf.nn[2];
-    for (int line = 0; line < 9; line++) {
-        const int fi = 2 * ic + line % 3 - 1, fj = 2 * jc + line / 3 - 1;
-        const bool ok = fi >= 0 && fi < gf.nn[0] && fj >= 0 && fj < gf.nn[1];
-        const TI* src = ok ? vf + nidx(gf, fi, fj, 0) * 3 : nullptr;
-        for (int t = threadIdx.x; t < L; t += blockDim.x) sl[line * L + t] = ok ? src[t] : TI(0);
-    }
-    __syncthreads();
-    const TA ti = (ic == 0 || ic == gc.nn[0] - 1) ? TA(1.0 / 1.5) : TA(0.5);
-    const TA tj = (jc == 0 || jc == gc.nn[1] - 1) ? TA(1.0 / 1.5) : TA(0.5);
-    for (int kc = threadIdx.x; kc < gc.nn[2]; kc += blockDim.x) {
-        const TA tk = (kc == 0 || kc == gc.nn[2] - 1) ? TA(1.0 / 1.5) : TA(0.5);
-        const int fk = 2 * kc;
-        const bool lo = fk - 1 >= 0, hi = fk + 1 < gf.nn[2];
-        TA acc[3] = {TA(0), TA(0), TA(0)};
-#pragma unroll
-        for (int dj = -1; dj <= 1; dj++) {
-            TA accj[3] = {TA(0), TA(0), TA(0)};
-#pragma unroll
-            for (int di = -1; di <= 1; di++) {
-                const TI* r = sl + ((dj + 1) * 3 + (di + 1)) * L;
-#pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    TA v = (TA)r[3 * fk + d];
-                    if (lo) v += TA(0.5) * (TA)r[3 * (fk - 1) + d];
-                    if (hi) v += TA(0.5) * (TA)r[3 * (fk + 1) + d];
-                    accj[d] += di == 0 ? v : TA(0.5) * v;
-                }
-            }
-#pragma unroll
-            for (int d = 0; d < 3; d++) acc[d] += dj == 0 ? accj[d] : TA(0.5) * accj[d];
-        }
-        const long long c = nidx(gc, ic, jc, kc);
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const TO bc = (TO)(acc[d] * ti * tj * tk);
-            vc[c * 3 + d] = bc;
-            if (j0.x) j0.x[c * 3 + d] = (TO)((*j0.omega) * j0.scale) * j0.dinv[c * 3 + d] * bc;
-        }
-    }
-}
-
 // 3D prolongation by cells: one thread per coarse node (ic, jc, kc) writes the up-to-8 fine
 // nodes (2ic + di, 2jc + dj, 2kc + dk), d in {0, 1}, from the up-to-8 coarse nodes
 // (ic + a, jc + b, kc + c).  Each coarse value is read once per thread instead of once per
@@ -307,11 +250,7 @@ int launch_restrict(const Grid& gf, const TI* vf, TO* vc, const int* skip, cudaS
     const Grid gc = coarse_grid(gf);
     const unsigned nb = (unsigned)((gc.n_nodes * gf.dim + 255) / 256);
     pf::count_launch();
-    const size_t lines_bytes = (size_t)9 * 3 * gf.nn[2] * sizeof(TI);
-    if (gf.dim == 3 && lines_bytes <= 48 * 1024)
-        PF_CUDA(launch_pdl(k_restrict_lines<TI, TO>, dim3((unsigned)(gc.nn[0] * gc.nn[1])), dim3(128), lines_bytes, st,
-                           gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0));
-    else if (gf.dim == 3)
+    if (gf.dim == 3)
         PF_CUDA(launch_pdl(k_restrict<3, TI, TO>, dim3(nb), dim3(256), 0, st, gdev<3>(gf), gdev<3>(gc), vf, vc, skip, j0));
     else
         PF_CUDA(launch_pdl(k_restrict<2, TI, TO>, dim3(nb), dim3(256), 0, st, gdev<2>(gf), gdev<2>(gc), vf, vc, skip, j0));
