@@ -280,7 +280,7 @@ def run_ours(args, rank, world, local_rank):
     avg_us = ms.value / max(n_l.value, 1) * 1e3
     achieved = byts.value / max(ms.value, 1e-12) / 1e6  # GB/s
     hbm, peak_kind = peaks()
-    kname = "k_matvec_h8p<float> / k_matvec_h8r<float>" if fp32 else "k_matvec_h8r<double>"
+    kname = "k_matvec_h8r<float>" if fp32 else "k_matvec_h8r<double>"
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
             "kernel": f"{kname} (fine-level stiffness matvec of the V-cycle, register x-march, fused epilogues)",
