@@ -129,6 +129,9 @@ typedef struct pf_mg_config {
     int coarse_op;      /* 0 = level 1 applied element by element from the fine densities when
                            K0 is an isotropic box element and level 1 is smoothed (else its
                            stencil); 1 = assembled stencils on every level */
+    unsigned w_mask;    /* bit l set: level l repeats its coarse correction from the updated
+                           iterate (the reference's lower-case 'w' cycle at the levels in
+                           w_level, _solvers.py:550-569); 0 = V-cycle */
 } pf_mg_config;
 
 typedef struct pf_solve_info {
@@ -144,8 +147,8 @@ int pf_mg_destroy(pf_mg* mg);
 /* Build D^-1, the Galerkin hierarchy and the coarse factor for densities E
  * (MultiGrid._setup, _solvers.py:442-516). */
 int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask, void* stream);
-/* z = V-cycle(r) from a zero initial guess with Jacobi weight omega (MultiGrid._multi_grid,
- * _solvers.py:518-571). */
+/* z = V-cycle(r) (W-cycle at the levels of cfg.w_mask) from a zero initial guess with
+ * Jacobi weight omega (MultiGrid._multi_grid, _solvers.py:518-571). */
 int pf_mg_vcycle(pf_mg* mg, const double* r, double* z, double omega, void* stream);
 /* PCG on K(E) x = b preconditioned by the V-cycle (MultiGrid.solve, _solvers.py:573-660).
  * Requires pf_mg_setup.  use_x0 != 0 starts from the contents of x, else from 0.
@@ -337,8 +340,8 @@ size_t pf_oc_multi_workspace_size(long long ne, int nm);
 int pf_oc_update_multi_f64(long long ne, int nm, const double* x, const double* df, const double* dg,
                            const double* h_vf, double move, double* x_new, double* work, double* h_out, void* stream);
 
-/* ---- PGD (pyFANTOM/Optimizers/CUDA/PGD.py:6-372), single volume constraint ---------- */
-size_t pf_pgd_workspace_size(long long n); /* doubles, for both calls below */
+/* ---- PGD (pyFANTOM/Optimizers/CUDA/PGD.py:6-372) --------------------------------------- */
+size_t pf_pgd_workspace_size(long long n); /* doubles, for the stats, step and single projection */
 /* h_out[8] (host) = {df.df, max|df|, df.df_last, df_last.df_last, s.y, s.s, y.y, max|y|}
  * with s = x_last - x, y = df_last - df (PGD.alpha, :107-142); x_last, df_last may both
  * be NULL (first iteration: entries 2..7 are 0). */
@@ -353,6 +356,17 @@ int pf_pgd_step_f64(long long n, const double* x, const double* df, const double
  * = {l, bisection steps, feasible at l = 0}. */
 int pf_pgd_project_f64(long long n, const double* xs, const double* dg, double vf, double lo, double hi, double tol,
                        double* x_new, double* work, double* h_out, void* stream);
+/* The same projection for one volume constraint per block of the design
+ * (project_to_feasible, :146-170 with m = nm > 1, the independent-constraints branch that
+ * MinimumCompliance takes for nm materials).  xs, x_new: nm blocks of ne; dg: nm blocks of
+ * ne, block c = row c of the constraint gradient on block c (MinimumCompliance's rows are
+ * zero elsewhere); h_vf (host): nm volume fractions.  The nm bisections run in lockstep
+ * while any block is unconverged (a block feasible at l = 0 keeps bisecting towards zero,
+ * about 1100 sweeps).  h_out (host, required) = {sweeps, feasible at l = 0 in every block,
+ * l_0 .. l_{nm-1}}.  1 <= nm <= 8; work: pf_pgd_multi_workspace_size(ne, nm) doubles. */
+size_t pf_pgd_multi_workspace_size(long long ne, int nm);
+int pf_pgd_project_multi_f64(long long ne, int nm, const double* xs, const double* dg, const double* h_vf, double lo,
+                             double hi, double tol, double* x_new, double* work, double* h_out, void* stream);
 
 /* ---- OC update without allocation --------------------------------------------------
  * No counterpart in the reference.  Same computation and outputs as pf_oc_update_f64,

@@ -67,6 +67,11 @@ def lib():
                                            ctypes.c_int, _dp]),
             "or_mg_vcycle": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, _dp, _dp, _bp, _dp, _dp]),
+            "or_mg_cycle": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_uint, _dp, _dp, _bp, _dp, _dp]),
+            "or_mgcg_solve_w": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                               _dp, _dp, _bp, _dp, _dp, ctypes.c_int, ctypes.c_uint, _dp, _ip]),
             "or_filter_normalizer": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp]),
             "or_filter_fwd": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp]),
             "or_filter_adj": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp, _dp]),
@@ -216,10 +221,12 @@ def stencil_to_dense(nel, A):
 
 
 def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega=0.4, omega_boost=1.06,
-               tol=1e-8, maxiter=1000, x0=None, deflation=None):
+               tol=1e-8, maxiter=1000, x0=None, deflation=None, w_level=()):
     """MultiGrid-preconditioned CG with the reference CUDA semantics.  ``deflation``: a
     nodal field whose components span a deflation space of the PCG (the library's learned
-    coarse-grid correction, pf_mg_set_deflation; no reference counterpart).
+    coarse-grid correction, pf_mg_set_deflation; no reference counterpart).  ``w_level``:
+    the levels where the reference's lower-case 'w' cycle applies its second coarse
+    correction (solvers/CUDA/_solvers.py:550-569); empty for the V-cycle.
 
     Returns (x, iterations, relative recursive residual, status)."""
     dim = len(nel)
@@ -232,7 +239,13 @@ def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega
     x = np.zeros(nd) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
     res = ctypes.c_double(0.0)
     st = ctypes.c_int(0)
-    if deflation is not None:
+    if w_level:
+        if deflation is not None:
+            raise ValueError("w_level and deflation together are not provided")
+        it = lib().or_mgcg_solve_w(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
+                                   pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None), _w_mask(w_level),
+                                   ctypes.byref(res), ctypes.byref(st))
+    elif deflation is not None:
         ya, py = _d(deflation)
         it = lib().or_mgcg_solve_deflated(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
                                           pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None), py,
@@ -282,8 +295,18 @@ def cg_solve(nel, K0, w, con, rhs, tol=1e-5, maxiter=1000, x0=None):
     return x, int(it), float(res.value)
 
 
-def mg_vcycle(nel, K0, w, con, r, n_level=3, n_smooth=2, omega=0.4, omega_boost=1.06):
-    """One V-cycle z = M r from a zero guess (level-0 Jacobi weight ``omega``)."""
+def _w_mask(w_level):
+    m = 0
+    for l in w_level:
+        if not 0 <= int(l) < 32:
+            raise ValueError(f"w_level {l} out of range")
+        m |= 1 << int(l)
+    return m
+
+
+def mg_vcycle(nel, K0, w, con, r, n_level=3, n_smooth=2, omega=0.4, omega_boost=1.06, w_level=()):
+    """One cycle z = M r from a zero guess (level-0 Jacobi weight ``omega``): the V-cycle,
+    or with ``w_level`` the lower-case 'w' cycle (second coarse correction at those levels)."""
     dim = len(nel)
     nd = n_nodes(nel) * dim
     nel_a, pn = _i(nel)
@@ -292,7 +315,8 @@ def mg_vcycle(nel, K0, w, con, r, n_level=3, n_smooth=2, omega=0.4, omega_boost=
     ca, pc = _con(con, nd)
     ra, pr = _d(r)
     z = np.zeros(nd)
-    st = lib().or_mg_vcycle(dim, pn, n_level, n_smooth, omega, omega_boost, pK, pw, pc, pr, z.ctypes.data_as(_dp))
+    st = lib().or_mg_cycle(dim, pn, n_level, n_smooth, omega, omega_boost, _w_mask(w_level), pK, pw, pc, pr,
+                           z.ctypes.data_as(_dp))
     if st:
         raise RuntimeError(f"coarse Cholesky failed at pivot {st}")
     return z
@@ -414,6 +438,36 @@ def pgd_project(xs, dg, vf, lo=0.0, hi=1.0, tol=1e-8):
             l1 = lm
         steps += 1
     return d, lm, steps
+
+
+def pgd_project_multi(xs, dg, vf, lo=0.0, hi=1.0, tol=1e-8):
+    """The reference PGD projection for m independent volume constraints, one per block of
+    the design (pyFANTOM/Optimizers/CPU/PGD.py:146-170 with m > 1; MinimumCompliance's
+    constraint rows are block-diagonal, Problem/CPU/MinimumCompliance.py:111-118).
+    xs (m, ne): the design by block; dg (m, ne): row i of the constraint gradient on
+    block i; vf (m,).  The m bisections run in lockstep: every sweep moves every shift to
+    its midpoint, and the sweeps continue while ANY block's (l2 - l1) / (l2 + l1) exceeds
+    tol (a block whose clip(xs) is feasible keeps l1 = 0, so its ratio stays 1 until l2
+    underflows to zero, about 1100 sweeps).  When clip(xs) is feasible in every block the
+    result is clip(xs).  Returns (x_new (m, ne), l (m,), sweeps)."""
+    xs, dg = np.asarray(xs, np.float64), np.asarray(dg, np.float64)
+    vf = np.asarray(vf, np.float64)
+    m = xs.shape[0]
+    d = np.clip(xs, lo, hi)
+    if np.all(np.einsum("ij,ij->i", dg, d) - vf <= 0.0):
+        return d, np.zeros(m), 0
+    l1, l2 = np.zeros(m), np.full(m, -1e12)
+    lm = np.zeros(m)
+    sweeps = 0
+    with np.errstate(invalid="ignore"):
+        while np.any((l2 - l1) / (l2 + l1) > tol):
+            lm = (l1 + l2) / 2
+            d = np.clip(xs + lm[:, None] * dg, lo, hi)
+            ok = np.einsum("ij,ij->i", dg, d) - vf <= 0.0
+            l2 = np.where(ok, lm, l2)
+            l1 = np.where(ok, l1, lm)
+            sweeps += 1
+    return d, lm, sweeps
 
 
 def penalize(rho, penalty=3.0, void=1e-9, E_mul=1.0, heavyside=False, beta=2.0, eta=0.5):

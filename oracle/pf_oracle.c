@@ -464,7 +464,9 @@ void or_stencil_to_dense(int dim, const int* nel_of_level, const double* A, doub
  *          coarse = Cholesky(A_L + 1e-6 I);
  *   V-cycle(x=0, b, l): n_smooth Jacobi sweeps with omega*1.06^l, r = b - A x, restrict,
  *          recurse from zero, prolong, n_smooth Jacobi sweeps on A e = r from the
- *          prolonged e, x += e  (the 'W' default behaves as a V-cycle, F10);
+ *          prolonged e, x += e  (the 'W' default behaves as a V-cycle);
+ *   the lower-case 'w' cycle (_solvers.py:550-569) repeats that coarse correction once
+ *          more, from the updated x, at every level l in w_level (bit l of w_mask);
  *   PCG: omega starts at min_omega; after each iteration
  *          omega = min_omega + d_omega/2 * exp(-500 (clip(R, tol, 0.1) - tol)).
  * ---------------------------------------------------------------------------------- */
@@ -479,6 +481,7 @@ typedef struct {
     double* Dinv[8];
     double* Lc;     /* coarse Cholesky factor */
     double omega_boost;
+    unsigned w_mask; /* levels that take the 'w' cycle's second coarse correction */
     double* tmp[8][5]; /* per level: 0 r, 1 b, 2 e, 3 Ax, 4 x */
 } mg_t;
 
@@ -513,20 +516,23 @@ static void vcycle(mg_t* m, int l, double* x, const double* b, double omega) {
     double wl = omega * pow(m->omega_boost, l);
     memset(x, 0, sizeof(double) * n);
     jacobi(m, l, x, b, wl, 1);
-    double* r = m->tmp[l][0];
-    double* Ax = m->tmp[l][3];
-    level_matvec(m, l, x, Ax);
+    const int passes = ((m->w_mask >> l) & 1u) ? 2 : 1;
+    for (int pass = 0; pass < passes; pass++) {
+        double* r = m->tmp[l][0];
+        double* Ax = m->tmp[l][3];
+        level_matvec(m, l, x, Ax);
 #pragma omp parallel for
-    for (long i = 0; i < n; i++) r[i] = b[i] - Ax[i];
-    double* rc = m->tmp[l + 1][1];
-    double* ec = m->tmp[l + 1][4];
-    or_restrict(m->dim, m->nel[l], r, rc);
-    vcycle(m, l + 1, ec, rc, omega);
-    double* e = m->tmp[l][2];
-    or_prolong(m->dim, m->nel[l], ec, e);
-    jacobi(m, l, e, r, wl, 0);
+        for (long i = 0; i < n; i++) r[i] = b[i] - Ax[i];
+        double* rc = m->tmp[l + 1][1];
+        double* ec = m->tmp[l + 1][4];
+        or_restrict(m->dim, m->nel[l], r, rc);
+        vcycle(m, l + 1, ec, rc, omega);
+        double* e = m->tmp[l][2];
+        or_prolong(m->dim, m->nel[l], ec, e);
+        jacobi(m, l, e, r, wl, 0);
 #pragma omp parallel for
-    for (long i = 0; i < n; i++) x[i] += e[i];
+        for (long i = 0; i < n; i++) x[i] += e[i];
+    }
 }
 
 /* deterministic dot product: 64 fixed chunks summed in order (an OpenMP reduction
@@ -547,8 +553,9 @@ static double dot(long n, const double* a, const double* b) {
 }
 
 static int mg_build(mg_t* m, int dim, const int* nel, int n_level, int n_smooth, double omega_boost,
-                    const double* K0, const double* w, const uint8_t* con) {
+                    const double* K0, const double* w, const uint8_t* con, unsigned w_mask) {
     memset(m, 0, sizeof(*m));
+    m->w_mask = w_mask;
     m->dim = dim;
     m->n_level = n_level;
     m->n_smooth = n_smooth;
@@ -595,10 +602,19 @@ static void mg_release(mg_t* m) {
 }
 
 /* One V-cycle z = M r from a zero guess with level-0 Jacobi weight omega. */
+int or_mg_cycle(int dim, const int* nel, int n_level, int n_smooth, double omega, double omega_boost,
+                unsigned w_mask, const double* K0, const double* w, const uint8_t* con, const double* r, double* z);
+
 int or_mg_vcycle(int dim, const int* nel, int n_level, int n_smooth, double omega, double omega_boost,
                  const double* K0, const double* w, const uint8_t* con, const double* r, double* z) {
+    return or_mg_cycle(dim, nel, n_level, n_smooth, omega, omega_boost, 0u, K0, w, con, r, z);
+}
+
+/* One cycle z = M r from a zero guess; w_mask: levels with the 'w' second correction */
+int or_mg_cycle(int dim, const int* nel, int n_level, int n_smooth, double omega, double omega_boost,
+                unsigned w_mask, const double* K0, const double* w, const uint8_t* con, const double* r, double* z) {
     mg_t m;
-    int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con);
+    int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con, w_mask);
     if (st == 0) vcycle(&m, 0, z, r, omega);
     mg_release(&m);
     return st;
@@ -690,10 +706,10 @@ static void defl_free(defl_t* d) {
 static int mgcg_core(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
                      double omega_boost, double tol, int maxiter, const double* K0, const double* w,
                      const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
-                     int* status_out, double* times_out, const double* Y) {
+                     int* status_out, double* times_out, const double* Y, unsigned w_mask) {
     mg_t m;
     const double t0 = wall_s();
-    int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con);
+    int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con, w_mask);
     const double t1 = wall_s();
     int iters = 0;
     double R = 0.0;
@@ -766,7 +782,7 @@ int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, doub
                         const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
                         int* status_out, double* times_out) {
     return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
-                     use_x0, res_out, status_out, times_out, NULL);
+                     use_x0, res_out, status_out, times_out, NULL, 0u);
 }
 
 /* or_mgcg_solve with the deflation space spanned by the components of the nodal field Y */
@@ -775,7 +791,16 @@ int or_mgcg_solve_deflated(int dim, const int* nel, int n_level, int n_smooth, d
                            const uint8_t* con, const double* rhs, double* x, int use_x0, const double* Y,
                            double* res_out, int* status_out) {
     return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
-                     use_x0, res_out, status_out, NULL, Y);
+                     use_x0, res_out, status_out, NULL, Y, 0u);
+}
+
+/* or_mgcg_solve with the 'w' cycle's second coarse correction at the levels of w_mask */
+int or_mgcg_solve_w(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                    double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                    const uint8_t* con, const double* rhs, double* x, int use_x0, unsigned w_mask, double* res_out,
+                    int* status_out) {
+    return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
+                     use_x0, res_out, status_out, NULL, NULL, w_mask);
 }
 
 int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,

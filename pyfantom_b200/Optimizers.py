@@ -16,6 +16,7 @@ import math
 import sys
 import time
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -130,15 +131,20 @@ class PGD(Optimizer):
     iteration: a Barzilai-Borwein step size from the gradient history with the reference's
     safeguards and fall-backs (PGD.alpha, :107-142), optionally along conjugate directions
     (beta = max(dx_n.(dx_n - dx_n-1) / |dx_n-1|^2, 0) with dx = -df), the step
-    x + alpha d, then the projection onto the volume constraint by the reference's bisection
-    for the shift l of clip(x + l dg, 0, 1) (:144-170).  The vector work runs in the
-    library (``pf_pgd_stats_f64``: the eight dot products and maxima of the step-size rule
-    in one pass; ``pf_pgd_step_f64``; ``pf_pgd_project_f64``: the bisection on the device,
-    five levels per sweep); the scalar rule is evaluated on the host exactly as written in
-    the reference.  Only the single-constraint path (``problem.m() == 1``, the reference's
-    ``is_independent or m == 1`` branch) is provided: the multi-constraint Newton /
-    Wolfe-line-search projection belongs to multi-material problems, which this library
-    does not build.
+    x + alpha d, then the projection onto the volume constraints by the reference's
+    bisection for the shifts l of clip(x + l dg, 0, 1) (:144-170).  The vector work runs in
+    the library (``pf_pgd_stats_f64``: the eight dot products and maxima of the step-size
+    rule in one pass; ``pf_pgd_step_f64``; ``pf_pgd_project_f64`` /
+    ``pf_pgd_project_multi_f64``: the bisection on the device, five levels per pass); the
+    scalar rule is evaluated on the host exactly as written in the reference.
+
+    The projection is the reference's ``is_independent or m == 1`` branch, which every
+    MinimumCompliance problem takes (``is_independent()`` is always true there): one
+    constraint, or one per material with the m shifts bisected in lockstep.  The m > 1
+    case needs constraint rows that are zero off their own block of the design, as
+    MinimumCompliance builds them.  The Newton / Wolfe-line-search branch for coupled
+    constraints (:172-210) serves problems whose ``is_independent()`` is false; no problem
+    of this library is one, and such a problem raises NotImplementedError.
     """
 
     def __init__(self, problem, change_tol=1e-4, fun_tol=1e-6, maxiter_N=50, tol_B=1e-8, tol_N=1e-6, C=1e12,
@@ -149,8 +155,12 @@ class PGD(Optimizer):
         self.last_f = problem.f()
         self.last_nabla_f = problem.nabla_f().clone()
         self.m = problem.m()
-        if self.m != 1:
-            raise NotImplementedError("PGD here supports a single volume constraint (problem.m() == 1)")
+        self.is_independent = problem.is_independent()
+        if self.m > 1 and not self.is_independent:
+            raise NotImplementedError("PGD here projects onto independent constraints (problem.is_independent())")
+        if self.m > 8:
+            raise NotImplementedError("PGD here projects onto at most 8 volume constraints")
+        self._blocks = None  # (dg, rows of dg on their own blocks) for m > 1
         self.lambda_map = problem.constraint_map()
         self.bounds = problem.bounds()
         self.change = float("inf")
@@ -168,7 +178,6 @@ class PGD(Optimizer):
         self.warmup_iter = warmup_iter
         self.conjugate = conjugate_directions
         self.iteration = 0
-        self.is_independent = problem.is_independent()
         self.d_last = None
         self.last_alpha = None
         self.last_projection = None
@@ -229,14 +238,48 @@ class PGD(Optimizer):
 
     def project_to_feasible(self, desvars_new, desvars, dg):
         n = desvars_new.shape[0]
-        out = (ctypes.c_double * 3)()
+        desvars_new = desvars_new.contiguous()
         x_new = torch.empty_like(desvars_new)
-        desvars_new, dg = desvars_new.contiguous(), dg.contiguous()
+        if self.m > 1:
+            return self._project_blocks(desvars_new, dg, x_new)
+        out = (ctypes.c_double * 3)()
+        dg = dg.contiguous()
         _lib.check(_lib.load().pf_pgd_project_f64(n, _lib.ptr(desvars_new), _lib.ptr(dg),
                                                   float(self.problem.volume_fraction), float(self.bounds[0]),
                                                   float(self.bounds[1]), float(self.tol_B), _lib.ptr(x_new),
                                                   _lib.ptr(self._ws(n)), out, _lib.stream()))
         self.last_projection = {"l": out[0], "steps": int(out[1]), "feasible_at_zero": bool(out[2])}
+        return x_new
+
+    def _project_blocks(self, desvars_new, dg, x_new):
+        """m volume constraints, row i of dg nonzero only on block i of the design."""
+        m = self.m
+        n = desvars_new.shape[0]
+        ne = n // m
+        if dg.dim() != 2 or tuple(dg.shape) != (m, n) or ne * m != n:
+            raise ValueError(f"nabla_g of shape {tuple(dg.shape)} for {m} constraints on {n} variables")
+        if self._blocks is None or self._blocks[0] is not dg:
+            rows = torch.stack([dg[i, i * ne:(i + 1) * ne] for i in range(m)]).contiguous()
+            if int(torch.count_nonzero(dg)) != int(torch.count_nonzero(rows)):
+                raise NotImplementedError("PGD here projects onto constraints with block-diagonal rows "
+                                          "(one volume constraint per material)")
+            self._blocks = (dg, rows)
+        rows = self._blocks[1]
+        vf = getattr(self.problem, "_vf_h", None)
+        if vf is None:
+            vf = self.problem.volume_fraction
+            vf = vf.cpu() if torch.is_tensor(vf) else vf
+        vf = np.broadcast_to(np.asarray(vf, dtype=np.float64), (m,)).copy()
+        lib = _lib.load()
+        need = int(lib.pf_pgd_multi_workspace_size(ne, m))
+        if self._work is None or self._work.numel() < need:
+            self._work = torch.empty(need, dtype=torch.float64, device=device())
+        out = (ctypes.c_double * (2 + m))()
+        _lib.check(lib.pf_pgd_project_multi_f64(ne, m, _lib.ptr(desvars_new), _lib.ptr(rows),
+                                                vf.ctypes.data_as(ctypes.c_void_p), float(self.bounds[0]),
+                                                float(self.bounds[1]), float(self.tol_B), _lib.ptr(x_new),
+                                                _lib.ptr(self._work), out, _lib.stream()))
+        self.last_projection = {"l": list(out[2:2 + m]), "steps": int(out[0]), "feasible_at_zero": bool(out[1])}
         return x_new
 
     def iter(self):

@@ -37,7 +37,8 @@ class pf_grid(ctypes.Structure):
 class pf_mg_config(ctypes.Structure):
     _fields_ = [("n_level", ctypes.c_int), ("n_smooth", ctypes.c_int), ("omega", ctypes.c_double),
                 ("min_omega", ctypes.c_double), ("omega_boost", ctypes.c_double), ("coarse_beta", ctypes.c_double),
-                ("precision", ctypes.c_int), ("check_every", ctypes.c_int), ("coarse_op", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("check_every", ctypes.c_int), ("coarse_op", ctypes.c_int),
+                ("w_mask", ctypes.c_uint)]
 
 
 class pf_solve_info(ctypes.Structure):
@@ -115,6 +116,8 @@ SIGNATURES = {
     "pf_pgd_stats_f64": (_I, [_LL, _P, _P, _P, _P, _P, _P, _P]),
     "pf_pgd_step_f64": (_I, [_LL, _P, _P, _P, _D, _D, _P, _P, _P]),
     "pf_pgd_project_f64": (_I, [_LL, _P, _P, _D, _D, _D, _D, _P, _P, _P, _P]),
+    "pf_pgd_multi_workspace_size": (_SZ, [_LL, _I]),
+    "pf_pgd_project_multi_f64": (_I, [_LL, _I, _P, _P, _P, _D, _D, _D, _P, _P, _P, _P]),
     "pf_cnn_conv3d_fwd_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P]),
     "pf_cnn_conv3d_bwd_data_f32": (_I, [_P, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P]),
     "pf_cnn_conv3d_fwd_tc": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _P]),

@@ -591,37 +591,41 @@ static int vcycle(pf_mg* mg, int l, const T* b0, T** res, double* dot_partials, 
         Tb = tmp;
     }
     T* R = (T*)L.r;
-    if ((s = level_matvec<T>(mg, l, X, make_epi<T>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, R, omega, scale, skip), st)))
-        return s;
-    Jacobi0<T> j0;
-    const bool fuse = l + 1 < mg->nlev;  // the coarsest level is solved directly
-    if (fuse) {
-        j0.x = (T*)mg->L[l + 1].x;
-        j0.dinv = (const T*)mg->L[l + 1].dinv;
-        j0.omega = omega;
-        j0.scale = pow(mg->cfg.omega_boost, l + 1);
-    }
-    if ((s = launch_restrict<T, T>(L.g, R, (T*)mg->L[l + 1].b, skip, st, j0))) return s;
-    T* ec;
-    if ((s = vcycle<T>(mg, l + 1, nullptr, &ec, nullptr, nullptr, st, fuse))) return s;
     T* Eb = (T*)L.e;
-    if ((s = launch_prolong<T>(L.g, ec, Eb, skip, st))) return s;
-    for (int k = 0; k < mg->cfg.n_smooth; k++) {
-        const bool last = k == mg->cfg.n_smooth - 1;
-        if (!last) {
-            if ((s = level_matvec<T>(mg, l, Eb, make_epi<T>(PF_EPI_JACOBI, R, Eb, dinv, nullptr, Tb, omega, scale, skip), st)))
-                return s;
-            T* tmp = Eb;
-            Eb = Tb;
-            Tb = tmp;
-        } else {
-            Epi<T> ep = make_epi<T>(PF_EPI_JACOBI_ADD, R, Eb, dinv, X, X, omega, scale, skip);
-            if (dot_partials) {
-                ep.dot_partial = dot_partials;
-                if constexpr (sizeof(T) == 8) ep.dot_a = (const T*)dot_a;
-                ep.dot_of_y = 0;
+    // the 'w' cycle repeats the coarse correction from the updated X at the levels of w_mask
+    const int passes = (l < 32 && ((mg->cfg.w_mask >> l) & 1u)) ? 2 : 1;
+    for (int pass = 0; pass < passes; pass++) {
+        if ((s = level_matvec<T>(mg, l, X, make_epi<T>(PF_EPI_RESID, b, nullptr, nullptr, nullptr, R, omega, scale, skip), st)))
+            return s;
+        Jacobi0<T> j0;
+        const bool fuse = l + 1 < mg->nlev;  // the coarsest level is solved directly
+        if (fuse) {
+            j0.x = (T*)mg->L[l + 1].x;
+            j0.dinv = (const T*)mg->L[l + 1].dinv;
+            j0.omega = omega;
+            j0.scale = pow(mg->cfg.omega_boost, l + 1);
+        }
+        if ((s = launch_restrict<T, T>(L.g, R, (T*)mg->L[l + 1].b, skip, st, j0))) return s;
+        T* ec;
+        if ((s = vcycle<T>(mg, l + 1, nullptr, &ec, nullptr, nullptr, st, fuse))) return s;
+        if ((s = launch_prolong<T>(L.g, ec, Eb, skip, st))) return s;
+        for (int k = 0; k < mg->cfg.n_smooth; k++) {
+            const bool last = k == mg->cfg.n_smooth - 1;
+            if (!last) {
+                if ((s = level_matvec<T>(mg, l, Eb, make_epi<T>(PF_EPI_JACOBI, R, Eb, dinv, nullptr, Tb, omega, scale, skip), st)))
+                    return s;
+                T* tmp = Eb;
+                Eb = Tb;
+                Tb = tmp;
+            } else {
+                Epi<T> ep = make_epi<T>(PF_EPI_JACOBI_ADD, R, Eb, dinv, X, X, omega, scale, skip);
+                if (dot_partials && pass == passes - 1) {
+                    ep.dot_partial = dot_partials;
+                    if constexpr (sizeof(T) == 8) ep.dot_a = (const T*)dot_a;
+                    ep.dot_of_y = 0;
+                }
+                if ((s = level_matvec<T>(mg, l, Eb, ep, st))) return s;
             }
-            if ((s = level_matvec<T>(mg, l, Eb, ep, st))) return s;
         }
     }
     *res = X;

@@ -5,7 +5,9 @@
   of K assembled dense on the device and factored by the library's tiled Cholesky
   (``pf_direct_solve_f64``, up to 20,480 free DOFs).
 * ``MultiGrid`` - geometric-multigrid-preconditioned CG (reference :330-660) with the
-  reference's V-cycle, damped-Jacobi smoother, adaptive omega schedule, Galerkin
+  reference's V-cycle (and its lower-case ``cycle='w'`` W-cycle, which repeats the coarse
+  correction at the levels in ``w_level``; the default ``'W'`` runs V-cycles there too),
+  damped-Jacobi smoother, adaptive omega schedule, Galerkin
   hierarchy and normalised transfers; the coarse solve is a dense Cholesky on the
   device instead of host CHOLMOD (every reference ``coarse_solver`` name maps to it,
   with the same ``beta = 1e-6`` shift).  Keyword-only extras: ``precision`` ('fp64',
@@ -181,10 +183,10 @@ class MultiGrid(Solver):
             raise ValueError("Coarse solver not recognized.")
         if matrix_free:
             raise NotImplementedError("Matrix free is not implemented yet.")
-        if cycle == "w":
-            # the reference only takes its W branch for a lower-case 'w'; the default 'W'
-            # runs V-cycles, which is what this solver implements
-            raise NotImplementedError("the lower-case 'w' (W-cycle) branch is not implemented; use 'V' or 'W'")
+        # the reference takes its second coarse correction only for a lower-case 'w'
+        # (_solvers.py:550); any other cycle name runs V-cycles
+        if cycle == "w" and any(not (0 <= int(l) < 32) for l in self.w_level):
+            raise ValueError("w_level entries must be levels 0..31")
         if precision not in ("fp64", "mixed", "mixed_bf16"):
             raise ValueError("precision must be 'fp64', 'mixed' or 'mixed_bf16'")
         if coarse_op not in ("auto", "element", "stencil"):
@@ -209,6 +211,7 @@ class MultiGrid(Solver):
         cfg.check_every = int(self.check_every)
         element = self.coarse_op == "element" or (self.coarse_op == "auto" and self.precision != "fp64")
         cfg.coarse_op = 0 if element else 1
+        cfg.w_mask = sum(1 << int(l) for l in set(self.w_level)) if self.cycle == "w" else 0
         h = ctypes.c_void_p()
         _lib.check(_lib.load().pf_mg_create(self.kernel._op, ctypes.byref(cfg), ctypes.byref(h)))
         self._mg = h

@@ -379,6 +379,73 @@ def pgd_goldens():
     return f
 
 
+class _FixedMultiProblem(_FixedProblem):
+    """_FixedProblem with one volume constraint per material block (dg of shape (m, m ne),
+    row i equal to 1/ne on block i, as MinimumCompliance builds it for m materials)."""
+
+    def __init__(self, x, vf, m):
+        super().__init__(x, np.zeros_like(x), np.asarray(vf, dtype=np.float64))
+        ne = x.size // m
+        self.dg = np.zeros((m, x.size))
+        for i in range(m):
+            self.dg[i, i * ne:(i + 1) * ne] = 1.0 / ne
+        self._m = m
+
+    def m(self):
+        return self._m
+
+    def g(self, rho=None):
+        r = self.x if rho is None else rho
+        return (self.dg @ r.reshape(-1, 1)).reshape(-1) - self.vf
+
+
+def pgd_multi_goldens():
+    """PGD with one volume constraint per material: the reference's projection
+    (project_to_feasible, the independent-constraints branch with m > 1) on stand-alone
+    cases, and 10 PGD iterations of the 2-material MBB half-beam (48x16, direct solve)."""
+    from pyFANTOM.Optimizers.CPU.PGD import PGD
+    rng = np.random.default_rng(29)
+    out = {}
+    # (tag, materials, elements per material, per-block (lo, hi) of the samples, volume fractions)
+    cases = [("q1", 2, 3000, [(0.2, 1.3), (-0.2, 1.2)], [0.3, 0.5]),
+             ("q2", 3, 2000, [(0.1, 1.1), (0.0, 0.3), (-0.3, 1.4)], [0.35, 0.5, 0.45]),
+             ("q3", 2, 1500, [(0.0, 0.4), (-0.5, 0.5)], [0.6, 0.4])]
+    for tag, m, ne, ranges, vf in cases:
+        xs = np.concatenate([rng.uniform(lo, hi, ne) for lo, hi in ranges])
+        fake = _FixedMultiProblem(np.clip(xs, 0, 1), vf, m)
+        q = PGD.__new__(PGD)
+        q.problem, q.is_independent, q.m, q.bounds, q.tol_B = fake, True, m, (0, 1.0), 1e-8
+        out[f"{tag}_xs"] = xs
+        out[f"{tag}_vf"] = np.array(vf)
+        out[f"{tag}_xnew"] = np.array(q.project_to_feasible(xs.copy(), xs.copy(), fake.dg))
+    wl = workloads.mbb2d(48, 16)
+    _, _, fe, _ = _simp_setup(wl, lambda m, k: SPSOLVE(k), 1.5, 0.3)
+    filt = StructuredFilter2D(fe.mesh, 1.5)
+    prob = MinimumCompliance(fe, filt, E_mul=[1.0, 0.5], void=1e-9, penalty=3.0, volume_fraction=[0.15, 0.15],
+                             heavyside=False)
+    t = time.time()
+    pgd = PGD(prob)  # initialises the design (uniform minimum volume fraction) and projects it
+    out["mbb_x_init"] = np.array(prob.get_desvars())
+    alphas = []
+    orig = pgd.alpha
+
+    def rec(*a):
+        r = orig(*a)
+        alphas.append(float(r[0]))
+        return r
+
+    pgd.alpha = rec
+    f = []
+    for it in range(10):
+        pgd.iter()
+        f.append(float(pgd.last_f))
+        if it in (0, 1, 9):
+            out[f"mbb_x{it + 1}"] = np.array(prob.get_desvars())
+    out.update(mbb_f=np.array(f), mbb_alpha=np.array(alphas), mbb_g10=np.array(prob.g()))
+    print(f"pgd multi-material: {time.time() - t:.1f}s f1={f[0]!r} f10={f[-1]!r}")
+    save("pgd_multi", **out)
+
+
 def sensitivity_goldens():
     """Compliance and its filtered sensitivity on a small bridge (direct solve)."""
     wl = workloads.bridge3d(12, 6, 6, seed=3)
@@ -460,6 +527,43 @@ def odd_goldens():
     out["mbb_r"] = r
     out["mbb_z"] = np.array(solver._multi_grid(np.zeros_like(r), r.copy(), 0))
     save("odd2d", **out)
+
+
+def wcycle_goldens():
+    """The lower-case 'w' cycle (solvers/CPU/_solvers.py _multi_grid, the second coarse
+    correction at the levels in w_level): one cycle from a zero guess with level-0 Jacobi
+    weight 0.45 for three w_level sets on a 16x8x8 cantilever (3 coarse levels), and
+    MultiGrid solves with cycle='w' there and on a 32x16 MBB beam."""
+    rng = np.random.default_rng(4242)
+    out = {}
+    wl = workloads.cantilever3d(16, 8, 8, seed=0)
+    for tag, wlev in [("w0", [0]), ("w1", [1]), ("w01", [0, 1])]:
+        fac = lambda m, k, wlev=wlev: MultiGrid(m, k, maxiter=500, tol=1e-10, n_smooth=2, omega=0.6,  # noqa: E731
+                                                n_level=3, cycle="w", w_level=wlev)
+        _, kern, fe, _ = _simp_setup(wl, fac, 2.0, 0.3)
+        U, res = fe.solve(wl["E"])
+        out[f"{tag}_U"] = np.array(U)
+        out[f"{tag}_res"] = np.array(res)
+        solver = fe.solver
+        r = rng.standard_normal(np.array(fe.rhs).shape[0])
+        r[np.nonzero(kern.constraints)[0]] = 0.0
+        solver.matrix_free = False
+        solver._setup()
+        solver.coarse_solve = solver._coarse_solver(solver.levels[-1][0])
+        solver.omega = 0.45
+        out[f"{tag}_r"] = r
+        out[f"{tag}_z"] = np.array(solver._multi_grid(np.zeros_like(r), r.copy(), 0))
+    out["E"] = wl["E"]
+    out["rhs"] = wl["rhs"]
+    wl2 = workloads.mbb2d(32, 16)
+    fac = lambda m, k: MultiGrid(m, k, maxiter=500, tol=1e-10, n_smooth=2, omega=0.6, n_level=3,  # noqa: E731
+                                 cycle="w", w_level=1)
+    _, kern, fe, _ = _simp_setup(wl2, fac, 1.5, 0.5)
+    U, res = fe.solve(wl2["E"])
+    out["mbb_U"] = np.array(U)
+    out["mbb_res"] = np.array(res)
+    out["mbb_E"] = wl2["E"]
+    save("wcycle", **out)
 
 
 def cg_goldens():

@@ -80,10 +80,7 @@ def test_two_material_oc_trajectory_matches_reference(golden):
 
 def test_single_material_paths_reject_multi():
     from pyfantom_b200.autograd import compliance
-    from pyfantom_b200.CUDA import PGD
     prob = _mbb_two_materials()
     prob.init_desvars()
-    with pytest.raises(NotImplementedError):
-        PGD(prob)
     with pytest.raises(NotImplementedError):
         compliance(prob.get_desvars(), prob)

@@ -176,6 +176,22 @@ def test_pgd_projection_matches_reference(golden, tag):
         assert steps > 20 and l < 0
 
 
+@pytest.mark.parametrize("tag,m", [("q1", 2), ("q2", 3), ("q3", 2)])
+def test_pgd_block_projection_matches_reference(golden, tag, m):
+    """m lockstep bisections, one per material block (the reference's m > 1 branch).  The
+    shifts are refined to the last bit of the constraint sums, summed here per block and in
+    the reference over the whole row, hence 1e-15 rather than equality."""
+    g = golden("pgd_multi")
+    xs = g[tag + "_xs"].reshape(m, -1)
+    ne = xs.shape[1]
+    x, l, sweeps = O.pgd_project_multi(xs, np.full((m, ne), 1.0 / ne), g[tag + "_vf"])
+    assert np.abs(x.reshape(-1) - g[tag + "_xnew"]).max() < 1e-15
+    if tag == "q3":  # clip(xs) satisfies every constraint
+        assert sweeps == 0 and np.all(l == 0.0)
+    else:  # one block feasible at l = 0: its l2 halves from -1e12 until it underflows
+        assert sweeps == 1115 and np.sum(l == 0.0) == 1 and np.all(l <= 0.0)
+
+
 def test_pgd_golden_trajectory_sane(golden):
     g = golden("pgd")
     f = g["f"]
@@ -265,3 +281,32 @@ def test_odd_2d_vcycle_matches_reference(golden):
                     omega=0.45)
     assert rel(z, g["mbb_z"]) < 1e-12
     assert float(g["mbb_res"]) > 1e-4
+
+
+@pytest.mark.parametrize("tag,w_level", [("w0", (0,)), ("w1", (1,)), ("w01", (0, 1))])
+def test_w_cycle_matches_reference(golden, tag, w_level):
+    """The lower-case 'w' cycle (a second coarse correction at the levels in w_level) on a
+    16x8x8 cantilever with 3 coarse levels: one cycle from a zero guess on the reference's
+    own hierarchy, and the MultiGrid solve to 1e-10."""
+    g = golden("wcycle")
+    nel = (16, 8, 8)
+    wl = workloads.cantilever3d(*nel, seed=0)
+    assert np.array_equal(wl["rhs"], g["rhs"]) and np.array_equal(wl["E"], g["E"])
+    K0 = unit_K0(3)
+    z = O.mg_vcycle(nel, K0, g["E"], wl["fixed_dofs"], g[tag + "_r"], n_level=3, n_smooth=2, omega=0.45,
+                    w_level=w_level)
+    assert rel(z, g[tag + "_z"]) < 1e-12
+    zv = O.mg_vcycle(nel, K0, g["E"], wl["fixed_dofs"], g[tag + "_r"], n_level=3, n_smooth=2, omega=0.45)
+    assert rel(zv, g[tag + "_z"]) > 1e-3  # the second correction changes the cycle
+    x, it, res, st = O.mgcg_solve(nel, K0, g["E"], wl["fixed_dofs"], g["rhs"], n_level=3, tol=1e-10,
+                                  w_level=w_level)
+    assert st == 0 and res < 1e-10
+    assert rel(x, g[tag + "_U"]) < 1e-8
+
+
+def test_w_cycle_2d_solve_matches_reference(golden):
+    g = golden("wcycle")
+    wl = workloads.mbb2d(32, 16)
+    x, it, res, st = O.mgcg_solve((32, 16), unit_K0(2), g["mbb_E"], wl["fixed_dofs"], wl["rhs"], n_level=3,
+                                  tol=1e-10, w_level=(1,))
+    assert st == 0 and rel(x, g["mbb_U"]) < 1e-8

@@ -100,3 +100,77 @@ def test_pgd_trajectory_matches_reference(golden):
     assert np.abs(prob.get_desvars().cpu().numpy() - g["x30"]).max() < 1e-5
     assert pgd.logs()["objective"] == pytest.approx(g["f"][-1], rel=1e-6)
     assert not pgd.converged() or pgd.change <= pgd.change_tol
+
+
+@pytest.mark.parametrize("tag,m", [("q1", 2), ("q2", 3), ("q3", 2)])
+def test_block_projection_matches_reference(golden, tag, m):
+    """One volume constraint per material block: the reference's lockstep bisection
+    (fixtures from its project_to_feasible with m > 1).  q1 and q2 hold a block that is
+    feasible at l = 0, which keeps the loop going until its l2 underflows (1115 sweeps);
+    q3 is feasible everywhere (clip(xs)).  The final shifts are refined to the last bit of
+    the constraint sums, whose order differs from the reference's, hence 1e-14 on x."""
+    g = golden("pgd_multi")
+    xs = g[tag + "_xs"]
+    ne = xs.size // m
+    vf = np.ascontiguousarray(g[tag + "_vf"], dtype=np.float64)
+    dgb = np.full((m, ne), 1.0 / ne)
+    xt = torch.as_tensor(xs, device="cuda")
+    dg = torch.as_tensor(dgb, device="cuda")
+    out = torch.empty_like(xt)
+    lib = _lib.load()
+    w = torch.empty(int(lib.pf_pgd_multi_workspace_size(ne, m)), dtype=torch.float64, device="cuda")
+    h = (ctypes.c_double * (2 + m))()
+    _lib.check(lib.pf_pgd_project_multi_f64(ne, m, _lib.ptr(xt), _lib.ptr(dg), vf.ctypes.data, 0.0, 1.0, 1e-8,
+                                            _lib.ptr(out), _lib.ptr(w), h, _lib.stream()))
+    x_ref, l_ref, sweeps_ref = O.pgd_project_multi(xs.reshape(m, ne), dgb, vf)
+    assert int(h[0]) == sweeps_ref and bool(h[1]) == (sweeps_ref == 0)
+    assert np.allclose(list(h)[2:], l_ref, rtol=1e-13, atol=0)
+    assert np.abs(out.cpu().numpy() - g[tag + "_xnew"]).max() < 1e-14
+    assert np.abs(out.cpu().numpy() - x_ref.reshape(-1)).max() < 1e-14
+    # no host buffer: refused (the sweep count is only known on the host)
+    assert lib.pf_pgd_project_multi_f64(ne, m, _lib.ptr(xt), _lib.ptr(dg), vf.ctypes.data, 0.0, 1.0, 1e-8,
+                                        _lib.ptr(out), _lib.ptr(w), None, _lib.stream()) == _lib.PF_BAD_ARG
+
+
+def test_block_projection_with_one_block_is_the_single_projection(golden):
+    g = golden("pgd")
+    xs = g["p2_xs"]
+    n = xs.size
+    vf = np.array([float(g["p2_vf"])])
+    xt = torch.as_tensor(xs, device="cuda")
+    dg = torch.full((n,), 1.0 / n, dtype=torch.float64, device="cuda")
+    lib = _lib.load()
+    a, b = torch.empty_like(xt), torch.empty_like(xt)
+    h1, h2 = (ctypes.c_double * 3)(), (ctypes.c_double * 3)()
+    _lib.check(lib.pf_pgd_project_f64(n, _lib.ptr(xt), _lib.ptr(dg), float(vf[0]), 0.0, 1.0, 1e-8, _lib.ptr(a),
+                                      _lib.ptr(_ws(n)), h1, _lib.stream()))
+    w = torch.empty(int(lib.pf_pgd_multi_workspace_size(n, 1)), dtype=torch.float64, device="cuda")
+    _lib.check(lib.pf_pgd_project_multi_f64(n, 1, _lib.ptr(xt), _lib.ptr(dg), vf.ctypes.data, 0.0, 1.0, 1e-8,
+                                            _lib.ptr(b), _lib.ptr(w), h2, _lib.stream()))
+    assert torch.equal(a, b) and h1[0] == h2[2] and h1[1] == h2[0]
+
+
+def test_two_material_pgd_trajectory_matches_reference(golden):
+    """PGD on the 2-material MBB half-beam (48x16, volume fractions 0.15 / 0.15) for 10
+    iterations against the reference's (direct solve there, MGCG to 1e-11 here)."""
+    from test_multimaterial_gpu import _mbb_two_materials
+    from pyfantom_b200.CUDA import PGD
+    g = golden("pgd_multi")
+    prob = _mbb_two_materials()
+    pgd = PGD(prob)
+    assert np.abs(prob.get_desvars().cpu().numpy() - g["mbb_x_init"]).max() < 1e-12
+    f, alpha = [], []
+    for it in range(10):
+        pgd.iter()
+        f.append(float(pgd.last_f))
+        alpha.append(pgd.last_alpha)
+        if it in (0, 1):
+            assert np.abs(prob.get_desvars().cpu().numpy() - g[f"mbb_x{it + 1}"]).max() < 1e-9
+    f, alpha = np.array(f), np.array(alpha)
+    assert abs(f[0] - g["mbb_f"][0]) < 1e-9 * g["mbb_f"][0]
+    assert np.abs(f - g["mbb_f"]).max() / g["mbb_f"].min() < 1e-6
+    ra = np.abs(alpha - g["mbb_alpha"]) / np.abs(g["mbb_alpha"])
+    assert ra[0] < 1e-9 and ra.max() < 1e-4, ra
+    assert np.abs(prob.get_desvars().cpu().numpy() - g["mbb_x10"]).max() < 1e-5
+    assert np.abs(prob.g().cpu().numpy() - g["mbb_g10"]).max() < 1e-8
+    assert len(pgd.last_projection["l"]) == 2

@@ -20,7 +20,7 @@ from pyfantom_b200 import workloads
 pytestmark = pytest.mark.gpu
 
 
-def setup_problem(wl, n_level, precision="fp64", tol=1e-10, maxiter=500, n_smooth=2, omega=0.6, solver="mg"):
+def setup_problem(wl, n_level, precision="fp64", tol=1e-10, maxiter=500, n_smooth=2, omega=0.6, solver="mg", **mg_kw):
     from pyfantom_b200.CUDA import (CG, FiniteElement, MultiGrid, StructuredMesh2D, StructuredMesh3D,
                                     StructuredStiffnessKernel)
     from pyfantom_b200.physics import LinearElasticity
@@ -30,7 +30,7 @@ def setup_problem(wl, n_level, precision="fp64", tol=1e-10, maxiter=500, n_smoot
     kern = StructuredStiffnessKernel(mesh)
     if solver == "mg":
         sol = MultiGrid(mesh, kern, maxiter=maxiter, tol=tol, n_smooth=n_smooth, omega=omega, n_level=n_level,
-                        precision=precision)
+                        precision=precision, **mg_kw)
     else:
         sol = CG(kern, maxiter=maxiter, tol=tol)
     fe = FiniteElement(mesh, kern, sol)
@@ -327,3 +327,53 @@ def test_odd_2d_vcycle_matches_reference_golden(golden):
     sol.setup()
     z = sol.vcycle(torch.as_tensor(g["mbb_r"], device="cuda"), omega=0.45).cpu().numpy()
     assert rel(z, g["mbb_z"]) < 1e-10
+
+
+@pytest.mark.parametrize("tag,w_level", [("w0", [0]), ("w1", [1]), ("w01", [0, 1])])
+def test_w_cycle_matches_reference_golden(golden, tag, w_level):
+    """The reference's lower-case 'w' cycle (second coarse correction at the levels in
+    w_level) on a 16x8x8 cantilever with 3 coarse levels: one cycle from a zero guess and
+    the MGCG solve to 1e-10 against the reference's own, the iteration count against the
+    oracle's."""
+    g = golden("wcycle")
+    nel = (16, 8, 8)
+    wl = workloads.cantilever3d(*nel, seed=0)
+    mesh, kern, sol, fe = setup_problem(wl, 3, cycle="w", w_level=w_level)
+    E = torch.as_tensor(g["E"], device="cuda")
+    kern.set_rho(E)
+    sol.setup()
+    z = sol.vcycle(torch.as_tensor(g[tag + "_r"], device="cuda"), omega=0.45).cpu().numpy()
+    assert rel(z, g[tag + "_z"]) < 1e-10
+    U, res = sol.solve(fe.rhs, rho=E, use_last=False)
+    x, it, _, _ = O.mgcg_solve(nel, unit_K0(3), g["E"], wl["fixed_dofs"], g["rhs"], n_level=3, tol=1e-10,
+                               w_level=w_level)
+    assert sol.last_info["status"] == "PF_OK" and abs(sol.last_info["iterations"] - it) <= 1
+    assert rel(U.cpu().numpy(), g[tag + "_U"]) < 1e-8
+    # the FP32 cycle (element-level level 1) with the same W levels reaches the same solution
+    mesh, kern, sol32, fe = setup_problem(wl, 3, precision="mixed", cycle="w", w_level=w_level)
+    U32, _ = sol32.solve(fe.rhs, rho=E, use_last=False)
+    assert sol32.last_info["status"] == "PF_OK" and rel(U32.cpu().numpy(), g[tag + "_U"]) < 1e-8
+    assert abs(sol32.last_info["iterations"] - it) <= 3
+
+
+def test_w_cycle_2d_matches_reference_golden(golden):
+    g = golden("wcycle")
+    wl = workloads.mbb2d(32, 16)
+    mesh, kern, sol, fe = setup_problem(wl, 3, cycle="w", w_level=1)
+    U, res = sol.solve(fe.rhs, rho=torch.as_tensor(g["mbb_E"], device="cuda"), use_last=False)
+    assert sol.last_info["status"] == "PF_OK" and rel(U.cpu().numpy(), g["mbb_U"]) < 1e-8
+
+
+def test_upper_case_w_runs_v_cycles(golden):
+    """Only the lower-case 'w' takes the second correction: 'W' (the default) and 'V' give
+    the V-cycle."""
+    g = golden("wcycle")
+    wl = workloads.cantilever3d(16, 8, 8, seed=0)
+    r = torch.as_tensor(g["w0_r"], device="cuda")
+    zs = []
+    for cyc in ("W", "V", "w"):
+        mesh, kern, sol, fe = setup_problem(wl, 3, cycle=cyc, w_level=0)
+        kern.set_rho(torch.as_tensor(g["E"], device="cuda"))
+        sol.setup()
+        zs.append(sol.vcycle(r, omega=0.45))
+    assert torch.equal(zs[0], zs[1]) and not torch.equal(zs[0], zs[2])
