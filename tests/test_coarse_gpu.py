@@ -39,7 +39,9 @@ def _solver(nel, E, cons, n_level, precision="fp64", coarse_op="element", K0=Non
 def _cases():
     rng = np.random.default_rng(11)
     out = []
-    for nel in [(8, 4, 4), (16, 8, 12), (12, 4, 64), (4, 64, 4), (24, 16, 124), (60, 8, 8)]:
+    # level-1 z extents 2 .. 70: one z-tile of the x-march (30 owned node columns), two (62) and
+    # three (70, the last partial)
+    for nel in [(8, 4, 4), (16, 8, 12), (12, 4, 64), (4, 64, 4), (24, 16, 124), (60, 8, 8), (8, 6, 140)]:
         n_nodes = int(np.prod(np.array(nel) + 1))
         out.append((nel, "cantilever", workloads.cantilever3d(*nel)["fixed_dofs"]))
         out.append((nel, "bridge", workloads.bridge3d(*nel)["fixed_dofs"]))

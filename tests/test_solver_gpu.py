@@ -44,23 +44,28 @@ def true_res(kern, U, rhs):
     return float(torch.linalg.norm(r) / torch.linalg.norm(rhs))
 
 
+# (16, 8, 40) and (12, 6, 70): two and three z-tiles of the fine matvec (30 owned node
+# columns each), the last one partial
 @pytest.mark.parametrize("case", [("cant", (16, 8, 8), 2), ("cant", (32, 16, 16), 3), ("bridge", (16, 8, 8), 3),
-                                  ("mbb", (64, 32), 3)])
-def test_vcycle_matches_oracle(case):
+                                  ("mbb", (64, 32), 3), ("cant", (16, 8, 40), 2), ("bridge", (12, 6, 70), 2)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_vcycle_matches_oracle(case, precision):
     kind, nel, nl = case
     wl = (workloads.cantilever3d(*nel) if kind == "cant" else workloads.bridge3d(*nel) if kind == "bridge"
           else workloads.mbb2d(*nel))
-    mesh, kern, sol, fe = setup_problem(wl, nl)
+    mesh, kern, sol, fe = setup_problem(wl, nl, precision=precision)
     kern.set_rho(torch.as_tensor(wl["E"], device="cuda"))
     sol.setup()
     r = np.random.default_rng(0).standard_normal(kern.shape[0])
     r[wl["fixed_dofs"]] = 0.0
     z = sol.vcycle(torch.as_tensor(r, device="cuda"), omega=0.45).cpu().numpy()
     zr = O.mg_vcycle(nel, unit_K0(len(nel)), wl["E"], wl["fixed_dofs"], r, n_level=nl, n_smooth=2, omega=0.45)
-    assert rel(z, zr) < 1e-10
+    # the FP32 cycle carries rounding of 1e-7 relative per operation; a wrong node (at a
+    # z-tile edge of the fine matvec, say) would be off by O(1)
+    assert rel(z, zr) < (1e-10 if precision == "fp64" else 1e-4)
 
 
-@pytest.mark.parametrize("case", [((16, 8, 8), 2), ((32, 16, 16), 3), ((24, 16, 8), 3)])
+@pytest.mark.parametrize("case", [((16, 8, 8), 2), ((32, 16, 16), 3), ((24, 16, 8), 3), ((16, 8, 40), 2)])
 def test_mgcg_matches_oracle(case):
     nel, nl = case
     wl = workloads.cantilever3d(*nel)
@@ -377,3 +382,4 @@ def test_upper_case_w_runs_v_cycles(golden):
         sol.setup()
         zs.append(sol.vcycle(r, omega=0.45))
     assert torch.equal(zs[0], zs[1]) and not torch.equal(zs[0], zs[2])
+
