@@ -132,6 +132,10 @@ typedef struct pf_mg_config {
     unsigned w_mask;    /* bit l set: level l repeats its coarse correction from the updated
                            iterate (the reference's lower-case 'w' cycle at the levels in
                            w_level, _solvers.py:550-569); 0 = V-cycle */
+    double omega_fixed; /* 0: the reference's Jacobi weight schedule (min_omega at the start,
+                           then min + (omega - min) / 2 exp(-500 (clip(R, tol, 0.1) - tol)));
+                           > 0: this weight in every V-cycle of the solve, a fixed
+                           preconditioner (no reference counterpart) */
 } pf_mg_config;
 
 typedef struct pf_solve_info {

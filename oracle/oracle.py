@@ -72,6 +72,10 @@ def lib():
             "or_mgcg_solve_w": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                _dp, _dp, _bp, _dp, _dp, ctypes.c_int, ctypes.c_uint, _dp, _ip]),
+            "or_mgcg_solve_ex": (ctypes.c_int, [ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                _dp, _dp, _bp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_uint,
+                                                ctypes.c_double, _dp, _ip]),
             "or_filter_normalizer": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp]),
             "or_filter_fwd": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp]),
             "or_filter_adj": (V, [ctypes.c_int, _ip, ctypes.c_int, _ip, _dp, _dp, _dp, _dp]),
@@ -221,12 +225,14 @@ def stencil_to_dense(nel, A):
 
 
 def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega=0.4, omega_boost=1.06,
-               tol=1e-8, maxiter=1000, x0=None, deflation=None, w_level=()):
+               tol=1e-8, maxiter=1000, x0=None, deflation=None, w_level=(), fixed_omega=None):
     """MultiGrid-preconditioned CG with the reference CUDA semantics.  ``deflation``: a
     nodal field whose components span a deflation space of the PCG (the library's learned
     coarse-grid correction, pf_mg_set_deflation; no reference counterpart).  ``w_level``:
     the levels where the reference's lower-case 'w' cycle applies its second coarse
-    correction (solvers/CUDA/_solvers.py:550-569); empty for the V-cycle.
+    correction (solvers/CUDA/_solvers.py:550-569); empty for the V-cycle.  ``fixed_omega``:
+    a Jacobi weight kept through the solve instead of the reference's schedule (the
+    library's option of the same name; no reference counterpart).
 
     Returns (x, iterations, relative recursive residual, status)."""
     dim = len(nel)
@@ -239,12 +245,11 @@ def mgcg_solve(nel, K0, w, con, rhs, n_level=3, n_smooth=2, omega=0.6, min_omega
     x = np.zeros(nd) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
     res = ctypes.c_double(0.0)
     st = ctypes.c_int(0)
-    if w_level:
-        if deflation is not None:
-            raise ValueError("w_level and deflation together are not provided")
-        it = lib().or_mgcg_solve_w(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
-                                   pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None), _w_mask(w_level),
-                                   ctypes.byref(res), ctypes.byref(st))
+    if w_level or fixed_omega is not None:
+        py = _d(deflation)[1] if deflation is not None else None
+        it = lib().or_mgcg_solve_ex(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,
+                                    pK, pw, pc, pr, x.ctypes.data_as(_dp), int(x0 is not None), py, _w_mask(w_level),
+                                    float(fixed_omega or 0.0), ctypes.byref(res), ctypes.byref(st))
     elif deflation is not None:
         ya, py = _d(deflation)
         it = lib().or_mgcg_solve_deflated(dim, pn, n_level, n_smooth, omega, min_omega, omega_boost, tol, maxiter,

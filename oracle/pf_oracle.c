@@ -468,7 +468,8 @@ void or_stencil_to_dense(int dim, const int* nel_of_level, const double* A, doub
  *   the lower-case 'w' cycle (_solvers.py:550-569) repeats that coarse correction once
  *          more, from the updated x, at every level l in w_level (bit l of w_mask);
  *   PCG: omega starts at min_omega; after each iteration
- *          omega = min_omega + d_omega/2 * exp(-500 (clip(R, tol, 0.1) - tol)).
+ *          omega = min_omega + d_omega/2 * exp(-500 (clip(R, tol, 0.1) - tol))
+ *          (or a fixed weight throughout: the library's fixed_omega option).
  * ---------------------------------------------------------------------------------- */
 typedef struct {
     int dim, n_level, n_smooth;
@@ -706,7 +707,7 @@ static void defl_free(defl_t* d) {
 static int mgcg_core(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
                      double omega_boost, double tol, int maxiter, const double* K0, const double* w,
                      const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
-                     int* status_out, double* times_out, const double* Y, unsigned w_mask) {
+                     int* status_out, double* times_out, const double* Y, unsigned w_mask, double fixed_omega) {
     mg_t m;
     const double t0 = wall_s();
     int st = mg_build(&m, dim, nel, n_level, n_smooth, omega_boost, K0, w, con, w_mask);
@@ -719,6 +720,10 @@ static int mgcg_core(int dim, const int* nel, int n_level, int n_smooth, double 
     } else {
         long n = m.ndof[0];
         double max_omega = omega, min_omega = fmax(omega / 2.0, min_omega_arg), d_omega = max_omega - min_omega;
+        if (fixed_omega > 0.0) { /* a fixed weight: the schedule's floor with no span */
+            min_omega = fixed_omega;
+            d_omega = 0.0;
+        }
         double cur = min_omega;
         double *r = (double*)malloc(sizeof(double) * n), *z = (double*)malloc(sizeof(double) * n);
         double *p = (double*)malloc(sizeof(double) * n), *q = (double*)malloc(sizeof(double) * n);
@@ -782,7 +787,7 @@ int or_mgcg_solve_timed(int dim, const int* nel, int n_level, int n_smooth, doub
                         const uint8_t* con, const double* rhs, double* x, int use_x0, double* res_out,
                         int* status_out, double* times_out) {
     return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
-                     use_x0, res_out, status_out, times_out, NULL, 0u);
+                     use_x0, res_out, status_out, times_out, NULL, 0u, 0.0);
 }
 
 /* or_mgcg_solve with the deflation space spanned by the components of the nodal field Y */
@@ -791,7 +796,7 @@ int or_mgcg_solve_deflated(int dim, const int* nel, int n_level, int n_smooth, d
                            const uint8_t* con, const double* rhs, double* x, int use_x0, const double* Y,
                            double* res_out, int* status_out) {
     return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
-                     use_x0, res_out, status_out, NULL, Y, 0u);
+                     use_x0, res_out, status_out, NULL, Y, 0u, 0.0);
 }
 
 /* or_mgcg_solve with the 'w' cycle's second coarse correction at the levels of w_mask */
@@ -800,7 +805,17 @@ int or_mgcg_solve_w(int dim, const int* nel, int n_level, int n_smooth, double o
                     const uint8_t* con, const double* rhs, double* x, int use_x0, unsigned w_mask, double* res_out,
                     int* status_out) {
     return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
-                     use_x0, res_out, status_out, NULL, NULL, w_mask);
+                     use_x0, res_out, status_out, NULL, NULL, w_mask, 0.0);
+}
+
+/* The general form: deflation field Y (may be NULL), 'w' cycle levels w_mask and a fixed
+ * Jacobi weight (fixed_omega > 0; 0 = the reference's schedule) */
+int or_mgcg_solve_ex(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,
+                     double omega_boost, double tol, int maxiter, const double* K0, const double* w,
+                     const uint8_t* con, const double* rhs, double* x, int use_x0, const double* Y, unsigned w_mask,
+                     double fixed_omega, double* res_out, int* status_out) {
+    return mgcg_core(dim, nel, n_level, n_smooth, omega, min_omega_arg, omega_boost, tol, maxiter, K0, w, con, rhs, x,
+                     use_x0, res_out, status_out, NULL, Y, w_mask, fixed_omega);
 }
 
 int or_mgcg_solve(int dim, const int* nel, int n_level, int n_smooth, double omega, double min_omega_arg,

@@ -38,7 +38,7 @@ class pf_mg_config(ctypes.Structure):
     _fields_ = [("n_level", ctypes.c_int), ("n_smooth", ctypes.c_int), ("omega", ctypes.c_double),
                 ("min_omega", ctypes.c_double), ("omega_boost", ctypes.c_double), ("coarse_beta", ctypes.c_double),
                 ("precision", ctypes.c_int), ("check_every", ctypes.c_int), ("coarse_op", ctypes.c_int),
-                ("w_mask", ctypes.c_uint)]
+                ("w_mask", ctypes.c_uint), ("omega_fixed", ctypes.c_double)]
 
 
 class pf_solve_info(ctypes.Structure):

@@ -7,7 +7,8 @@
 //           omega * boost^l, residual, restrict, recurse, prolong, n_smooth sweeps on
 //           A e = r starting from the prolonged e, x += e;
 //   PCG     omega starts at min_omega and after each iteration becomes
-//           min_omega + (omega - min_omega)/2 * exp(-500 (clip(R, tol, 0.1) - tol)),
+//           min_omega + (omega - min_omega)/2 * exp(-500 (clip(R, tol, 0.1) - tol))
+//           (or stays at cfg.omega_fixed: a fixed preconditioner, no reference counterpart),
 //           Fletcher-Reeves beta, stop when ||r||/||b|| < tol.
 // Differences of form, not of result: every scalar (alpha, beta, omega, ||r||) lives in
 // device memory and is consumed by the next kernel, so iterations are enqueued without
@@ -704,6 +705,10 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
         delete mg;
         return fail(PF_BAD_ARG, "coarse_op must be 0 (element operator on level 1 when available) or 1 (stencils)");
     }
+    if (!(cfg->omega_fixed >= 0.0) || !(cfg->omega_fixed < 2.0)) {
+        delete mg;
+        return fail(PF_BAD_ARG, "omega_fixed must be 0 (the reference schedule) or a Jacobi weight in (0, 2)");
+    }
     // level 1 element by element when it is smoothed (not the coarsest), its coarse elements
     // cover the fine grid (even element counts) and K0 allows it
     const bool even = g.nel[0] % 2 == 0 && g.nel[1] % 2 == 0 && (g.dim == 2 || g.nel[2] % 2 == 0);
@@ -890,10 +895,12 @@ __global__ void k_init_state(PcgState* st, double tol, int maxiter, double min_o
 }
 
 static int init_state(pf_mg* mg, double tol, int maxiter, double omega, cudaStream_t st) {
-    const double min_omega = fmax(mg->cfg.omega / 2.0, mg->cfg.min_omega);
+    // the schedule's floor and span; a fixed weight is a floor with no span
+    const bool fixed = mg->cfg.omega_fixed > 0.0;
+    const double min_omega = fixed ? mg->cfg.omega_fixed : fmax(mg->cfg.omega / 2.0, mg->cfg.min_omega);
+    const double d_omega = fixed ? 0.0 : mg->cfg.omega - min_omega;
     pf::count_launch();
-    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, mg->st, tol, maxiter, min_omega, mg->cfg.omega - min_omega, omega,
-                       0));
+    PF_CUDA(launch_pdl(k_init_state, dim3(1), dim3(1), 0, st, mg->st, tol, maxiter, min_omega, d_omega, omega, 0));
     PF_LAUNCH_CHECK("state init");
     return PF_OK;
 }

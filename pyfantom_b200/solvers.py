@@ -21,7 +21,9 @@
   than the FP32 stencil, and the stencil in the FP64 form, where the stencil is faster)
   and ``coarse_correction`` (an object with ``field(kernel, rhs)``, e.g.
   learned.LearnedCoarseSpace, whose nodal field spans a deflation space of the PCG,
-  ``pf_mg_set_deflation``).
+  ``pf_mg_set_deflation``) and ``fixed_omega`` (None: the reference's residual-driven
+  Jacobi weight, which changes the preconditioner from one iteration to the next; a
+  number: that weight in every V-cycle, a fixed preconditioner as PCG assumes).
 
 ``solve(rhs, rho=None, use_last=True)`` returns ``(U, residual)`` like the reference;
 ``last_x0`` holds the warm start.  Solver statistics of the last call are in
@@ -153,7 +155,7 @@ class MultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="cholmod", matrix_free=False, low_level_tol=1e-8,
                  low_level_maxiter=5000, min_omega=0.4, omega_boost=1.06, *, precision="fp64", check_every=4,
-                 warm_start=None, coarse_op="auto", coarse_correction=None):
+                 warm_start=None, coarse_op="auto", coarse_correction=None, fixed_omega=None):
         self.kernel = kernel
         self.warm_start = warm_start
         self.coarse_correction = coarse_correction
@@ -192,6 +194,9 @@ class MultiGrid(Solver):
         if coarse_op not in ("auto", "element", "stencil"):
             raise ValueError("coarse_op must be 'auto', 'element' or 'stencil'")
         self.coarse_op = coarse_op
+        if fixed_omega is not None and not (0.0 < float(fixed_omega) < 2.0):
+            raise ValueError("fixed_omega must be a Jacobi weight in (0, 2) or None")
+        self.fixed_omega = None if fixed_omega is None else float(fixed_omega)
         self._min_omega_arg = min_omega
         self._mg = None
         self._side = None
@@ -212,6 +217,7 @@ class MultiGrid(Solver):
         element = self.coarse_op == "element" or (self.coarse_op == "auto" and self.precision != "fp64")
         cfg.coarse_op = 0 if element else 1
         cfg.w_mask = sum(1 << int(l) for l in set(self.w_level)) if self.cycle == "w" else 0
+        cfg.omega_fixed = 0.0 if self.fixed_omega is None else self.fixed_omega
         h = ctypes.c_void_p()
         _lib.check(_lib.load().pf_mg_create(self.kernel._op, ctypes.byref(cfg), ctypes.byref(h)))
         self._mg = h
