@@ -416,7 +416,6 @@ __global__ void __launch_bounds__(576) k_dirty_walsh(const double* __restrict__ 
 // ---------------------------------------------------------------------------------------
 // matvec: register x-march over coarse elements
 // ---------------------------------------------------------------------------------------
-constexpr int kCZTile = 30;
 
 template <typename T>
 __device__ __forceinline__ T inv_tw(int n, int nn) {
@@ -523,7 +522,10 @@ __device__ __forceinline__ void coarse_ident(int x, int y, int z, int nx, int ny
     for (int a = 0; a < 3; a++) out[a] = acc[a];
 }
 
-template <typename T, int NW, int MINB, int MODE>
+// RW element rows per warp: lanes are RW segments of L = 32 / RW along z (shuffles of width L),
+// so a z-tile owns L - 2 node columns; RW = 2 wastes fewer lanes when the level's z extent
+// is just above a multiple of 30 (level 1 of a 256x128x128 grid: 65 node columns).
+template <typename T, int NW, int MINB, int MODE, int RW>
 __global__ void __launch_bounds__(NW * 32, MINB)
     k_coarse_matvec(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const T* __restrict__ Eh,
                     const T* __restrict__ Wd, const int* __restrict__ dlist, int cap, const CoarseCoef<T> cf,
@@ -531,20 +533,20 @@ __global__ void __launch_bounds__(NW * 32, MINB)
                     const T* __restrict__ S, int icap) {
     pdl_wait();
     pdl_trigger();
-    constexpr int TY = NW - 1;
+    constexpr int L = 32 / RW, NR = NW * RW, TY = NR - 1;  // lanes per row, rows, owned rows
     constexpr unsigned FULL = 0xffffffffu;
-    __shared__ T s_q[2][3][NW][32];
+    __shared__ T s_q[2][3][NR][L];
     if (epi.skip && *epi.skip) return;
     constexpr bool need_b = MODE != PF_EPI_STORE, need_x = MODE == PF_EPI_JACOBI || MODE == PF_EPI_JACOBI_ADD;
     constexpr bool need_xa = MODE == PF_EPI_JACOBI_ADD;
     const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
-    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int kz0 = blockIdx.x * kCZTile, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
+    const int tid = threadIdx.x, w = (tid >> 5) * RW + (tid & 31) / L, l = tid % L;  // w: row, l: lane in row
+    const int kz0 = blockIdx.x * (L - 2), jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
     const int je = jy0 - 1 + w, kc = kz0 - 1 + l;
     const bool col_ok = kc >= 0 && kc < nz;
     const bool ok0 = col_ok && je >= 0 && je < ny, ok1 = col_ok && je + 1 < ny;
-    const bool elem_ok = l < 31 && je >= 0 && je < NY && kc >= 0 && kc < NZ;
-    const bool owner = w < TY && l < kCZTile && je + 1 < ny && kc + 1 < nz;
+    const bool elem_ok = l < L - 1 && je >= 0 && je < NY && kc >= 0 && kc < NZ;
+    const bool owner = w < TY && l < L - 2 && je + 1 < ny && kc + 1 < nz;
     const int rows = nz * nx;
     const int n0 = kc + rows * je;
     const int n1 = n0 + rows;
@@ -579,7 +581,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const T s = v[1][c] + v[0][c], dd = v[1][c] - v[0][c];
-            const T sn = __shfl_down_sync(FULL, s, 1), dn = __shfl_down_sync(FULL, dd, 1);
+            const T sn = __shfl_down_sync(FULL, s, 1, L), dn = __shfl_down_sync(FULL, dd, 1, L);
             g[c][0][0] = s + sn;
             g[c][0][1] = sn - s;
             g[c][1][0] = dd + dn;
@@ -635,8 +637,8 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             const T r0a = G[c][0][0] - G[c][1][0], r0b = G[c][0][1] - G[c][1][1];
             const T r1a = G[c][0][0] + G[c][1][0], r1b = G[c][0][1] + G[c][1][1];
             const T lo0 = r0a - r0b, up0 = r0a + r0b, lo1 = r1a - r1b, up1 = r1a + r1b;
-            P1[c] = up1 + __shfl_down_sync(FULL, lo1, 1);
-            s_q[s & 1][c][w][l] = up0 + __shfl_down_sync(FULL, lo0, 1);
+            P1[c] = up1 + __shfl_down_sync(FULL, lo1, 1, L);
+            s_q[s & 1][c][w][l] = up0 + __shfl_down_sync(FULL, lo0, 1, L);
         }
         __syncthreads();
         if (out_now) {
@@ -693,11 +695,30 @@ struct CoarseShape {  // warps per block (NW - 1 owned element rows) and blocks 
     static constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
 };
 
+// element rows per warp (1 or 2): the one with fewer warp-rows of lanes per x-plane
 template <typename T>
-static void coarse_launch_dims(const Grid& g, dim3* grid, int* CXc) {
+static int coarse_rows_per_warp(const Grid& g) {
+    if (sizeof(T) != 4) return 1;
+    constexpr int NW = CoarseShape<T>::NW;
+    long long best = -1;
+    int pick = 1;
+    for (int rw = 1; rw <= 2; rw++) {
+        const int L = 32 / rw, nr = NW * rw;
+        const long long cost = (long long)((g.nn[2] + L - 3) / (L - 2)) * ((g.nn[1] + nr - 2) / (nr - 1)) * NW;
+        if (best < 0 || cost < best) {
+            best = cost;
+            pick = rw;
+        }
+    }
+    return pick;
+}
+
+template <typename T>
+static void coarse_launch_dims(const Grid& g, dim3* grid, int* CXc, int rw) {
     constexpr int NW = CoarseShape<T>::NW;
     const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
-    const int tz = (nz + kCZTile - 1) / kCZTile, ty = (ny + NW - 2) / (NW - 1);
+    const int L = 32 / rw, nr = NW * rw;
+    const int tz = (nz + L - 3) / (L - 2), ty = (ny + nr - 2) / (nr - 1);
     const long long slots = (long long)kNumSM * CoarseShape<T>::MINB;
     const long long cols = (long long)tz * ty;
     int best = 2;
@@ -714,12 +735,12 @@ static void coarse_launch_dims(const Grid& g, dim3* grid, int* CXc) {
     *grid = dim3(tz, ty, (nx + best - 1) / best);
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, int RW>
 static int coarse_launch(dim3 grid, int cx, const Grid& g, const T* u, const CoarseOp* c, const CoarseCoef<T>& cf,
                          const Epi<T>& epi, cudaStream_t st) {
     constexpr int NW = CoarseShape<T>::NW, MINB = CoarseShape<T>::MINB;
     const uint8_t* nflag = c->nident > 0 ? c->nflag : nullptr;
-    PF_CUDA(launch_pdl(k_coarse_matvec<T, NW, MINB, MODE>, grid, dim3(NW * 32), 0, st, g.nel[0], g.nel[1],
+    PF_CUDA(launch_pdl(k_coarse_matvec<T, NW, MINB, MODE, RW>, grid, dim3(NW * 32), 0, st, g.nel[0], g.nel[1],
                        g.nel[2], cx, u, (const T*)c->Eh, (const T*)c->Wd, (const int*)c->dlist, c->cap, cf, epi,
                        nflag, (const int*)c->nmap, (const T*)c->S, c->icap));
     return PF_OK;
@@ -730,20 +751,25 @@ int launch_coarse_matvec(const CoarseOp* c, const Grid& g, const T* u, const Epi
     if (epi.dot_partial) return fail(PF_UNSUPPORTED, "coarse element matvec: no fused dot");
     CoarseCoef<T> cf;
     for (int q = 0; q < kCoarseCoefs; q++) cf.b[q] = (T)c->coef[q];
+    const int rw = coarse_rows_per_warp<T>(g);
     dim3 grid;
     int cx;
-    coarse_launch_dims<T>(g, &grid, &cx);
+    coarse_launch_dims<T>(g, &grid, &cx, rw);
     pf::count_launch();
+#define PF_COARSE(M)                                                               \
+    return rw == 2 ? coarse_launch<T, M, sizeof(T) == 4 ? 2 : 1>(grid, cx, g, u, c, cf, epi, st) \
+                   : coarse_launch<T, M, 1>(grid, cx, g, u, c, cf, epi, st)
     switch (epi.mode) {
         case PF_EPI_STORE:
-            return coarse_launch<T, PF_EPI_STORE>(grid, cx, g, u, c, cf, epi, st);
+            PF_COARSE(PF_EPI_STORE);
         case PF_EPI_RESID:
-            return coarse_launch<T, PF_EPI_RESID>(grid, cx, g, u, c, cf, epi, st);
+            PF_COARSE(PF_EPI_RESID);
         case PF_EPI_JACOBI:
-            return coarse_launch<T, PF_EPI_JACOBI>(grid, cx, g, u, c, cf, epi, st);
+            PF_COARSE(PF_EPI_JACOBI);
         default:
-            return coarse_launch<T, PF_EPI_JACOBI_ADD>(grid, cx, g, u, c, cf, epi, st);
+            PF_COARSE(PF_EPI_JACOBI_ADD);
     }
+#undef PF_COARSE
 }
 template int launch_coarse_matvec<double>(const CoarseOp*, const Grid&, const double*, const Epi<double>&,
                                           cudaStream_t);
