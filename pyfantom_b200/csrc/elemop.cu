@@ -153,7 +153,17 @@ struct H8Coef {
 // loaded straight into its register once the current one is spent.  (Unrolling the march by
 // two to alternate register sets, or prefetching two planes ahead, measured slower: more
 // registers, fewer resident warps.)
+// Remainder z-tile: when the last z-tile holds at most 14 node columns (129 = 4 x 30 + 9
+// columns at 256x128x128, 97 = 3 x 30 + 7 at 192x96x96) its blocks split every warp into two
+// 16-lane segments, each computing its own element row (shuffles of width 16, 14 owned
+// columns per segment), so that tile costs half the warp-steps of a full-width one.  Blocks
+// 0 .. tzA * tyA - 1 are full-width tiles (z-tile b % tzA, y-tile b / tzA); the blocks after
+// them are the half-width y-tiles of the z-tile starting at column tzA * 30.
 constexpr int kZTileR = 30;
+struct H8Tiles {
+    int tzA, tyA;  // full-width z-tiles and y-tiles
+    int ncols;     // tile columns: tzA * tyA full-width, then the half-width ones
+};
 
 // element scale in the operator precision (E stored in FP64, FP32 or BF16)
 template <typename T, typename TE>
@@ -357,13 +367,13 @@ __device__ __forceinline__ void h8_element(const T (&glo)[3][2][2], const T (&gh
 
 template <typename T, typename TE, int NW, int MINB, int CM, int MODE, bool DOT>
 __global__ void __launch_bounds__(NW * 32, MINB)
-    k_matvec_h8r(int NX, int NY, int NZ, int CXc, const T* __restrict__ u, const TE* __restrict__ E,
+    k_matvec_h8r(int NX, int NY, int NZ, H8Tiles tl, const T* __restrict__ u, const TE* __restrict__ E,
                  const uint8_t* __restrict__ mask, const H8Blk<T> blk, const H8Coef<T> cf, Epi<T> epi) {
     pdl_wait();
     pdl_trigger();
-    constexpr int TY = NW - 1, NT = NW * 32;
+    constexpr int NT = NW * 32;
     constexpr unsigned FULL = 0xffffffffu;
-    __shared__ T s_q[2][3][NW][32];
+    __shared__ T s_q[2][3][NW * 32];  // [w * L + l]
     __shared__ double s_red[NW];
     __shared__ T s_blk[72];
     if (epi.skip && *epi.skip) return;
@@ -371,13 +381,34 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     constexpr bool need_b = mode != PF_EPI_STORE, need_x = mode == PF_EPI_JACOBI || mode == PF_EPI_JACOBI_ADD;
     constexpr bool need_xa = mode == PF_EPI_JACOBI_ADD;
     const int nx = NX + 1, ny = NY + 1, nz = NZ + 1;
-    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int kz0 = blockIdx.x * kZTileR, jy0 = blockIdx.y * TY, ix0 = blockIdx.z * CXc;
+    const int tid = threadIdx.x;
+    double dot = 0.0;
+    if (CM == 0 && tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
+    if (CM == 0) __syncthreads();
+    const volatile T* vb = s_blk;
+    // this block's share of the (tile column, node plane) work, node planes contiguous within
+    // a column: one march per column segment
+    const long long total = (long long)tl.ncols * nx;
+    long long wpos = total * blockIdx.x / gridDim.x;
+    const long long wend = total * (blockIdx.x + 1) / gridDim.x;
+    for (int seg = 0; wpos < wend; seg++) {
+    const int col = (int)(wpos / nx), ix0 = (int)(wpos % nx);
+    const int CXc = (int)min(wend - wpos, (long long)(nx - ix0));  // node planes ix0 .. ix0 + CXc - 1
+    wpos += CXc;
+    if (seg > 0) __syncthreads();  // the previous segment's last row exchange is read
+    // block-uniform tile shape: L lanes per element row (32, or 16 in the remainder z-tile)
+    const int bA = tl.tzA * tl.tyA;
+    const bool half = col >= bA;
+    const int L = half ? 16 : 32, TY = (half ? 2 * NW : NW) - 1;
+    const int w = half ? tid >> 4 : tid >> 5, l = tid & (L - 1);
+    const int zt = half ? tl.tzA : col % max(tl.tzA, 1);
+    const int yt = half ? col - bA : col / max(tl.tzA, 1);
+    const int kz0 = zt * kZTileR, jy0 = yt * TY;
     const int je = jy0 - 1 + w, kc = kz0 - 1 + l;  // element row; node column of its lower z corner
     const bool col_ok = kc >= 0 && kc < nz;
     const bool ok0 = col_ok && je >= 0 && je < ny, ok1 = col_ok && je + 1 < ny;
-    const bool elem_ok = l < 31 && je >= 0 && je < NY && kc >= 0 && kc < NZ;
-    const bool owner = w < TY && l < kZTileR && je + 1 < ny && kc + 1 < nz;
+    const bool elem_ok = l < L - 1 && je >= 0 && je < NY && kc >= 0 && kc < NZ;
+    const bool owner = w < TY && l < L - 2 && je + 1 < ny && kc + 1 < nz;
     // 32-bit node and element indices (grid validation keeps 3 * nodes below 2^31)
     const int rows = nz * nx;        // nodes per node row (y)
     const int n0 = kc + rows * je;   // node (je, 0, kc): rows je, je + 1 advance by nz per plane
@@ -386,9 +417,6 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     const int e0 = je * NZ + kc;     // element (0, je, kc)
     const bool has_mask = mask != nullptr;
     const T wgt = epi_omega(epi);
-    double dot = 0.0;
-    if (CM == 0 && tid < 72) s_blk[tid] = blk.b[tid / 9][(tid / 3) % 3][tid % 3];
-    const volatile T* vb = s_blk;
 
     // node values of this lane's column in rows je, je+1 of plane p (zero outside the mesh)
     // and the two constraint bytes; nothing here waits for the loads
@@ -426,7 +454,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const T s = v[1][c] + v[0][c], d = v[1][c] - v[0][c];
-            const T sn = __shfl_down_sync(FULL, s, 1), dn = __shfl_down_sync(FULL, d, 1);
+            const T sn = __shfl_down_sync(FULL, s, 1, L), dn = __shfl_down_sync(FULL, d, 1, L);
             g[c][0][0] = s + sn;
             g[c][0][1] = sn - s;
             g[c][1][0] = d + dn;
@@ -477,14 +505,14 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             const T r0a = G[c][0][0] - G[c][1][0], r0b = G[c][0][1] - G[c][1][1];
             const T r1a = G[c][0][0] + G[c][1][0], r1b = G[c][0][1] + G[c][1][1];
             const T lo0 = r0a - r0b, up0 = r0a + r0b, lo1 = r1a - r1b, up1 = r1a + r1b;
-            P1[c] = up1 + __shfl_down_sync(FULL, lo1, 1);
-            s_q[s & 1][c][w][l] = up0 + __shfl_down_sync(FULL, lo0, 1);
+            P1[c] = up1 + __shfl_down_sync(FULL, lo1, 1, L);
+            s_q[s & 1][c][w * L + l] = up0 + __shfl_down_sync(FULL, lo0, 1, L);
         }
         __syncthreads();
         if (out_now) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                T y = P1[c] + s_q[s & 1][c][w + 1][l];
+                T y = P1[c] + s_q[s & 1][c][(w + 1) * L + l];
                 if ((mo >> c) & 1) y = u[3 * no + c];
                 T o = y;
                 if constexpr (mode == PF_EPI_RESID) {
@@ -513,7 +541,6 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
             for (int b = 0; b < 2; b++) carry[c][a][b] = T(0);
     T eA = escale(ix0 - 1);
-    if (CM == 0) __syncthreads();
     for (int s = 0; s <= CXc; s++) {
         step(s, gA, gB, vA, mA0, mA1, eA);
         // the upper face becomes the next lower face (computed values: no wait)
@@ -524,10 +551,10 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
                 for (int b = 0; b < 2; b++) gA[c][a][b] = gB[c][a][b];
     }
+    }  // column segments
     if constexpr (DOT) {
         const double sblk = block_sum<NT>(dot, s_red);
-        if (threadIdx.x == 0)
-            epi.dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = sblk;
+        if (threadIdx.x == 0) epi.dot_partial[blockIdx.x] = sblk;
     }
 }
 
@@ -750,32 +777,32 @@ static H8Blk<T> make_blk(const Op* op) {
 // FP32 with 9 warps x 3 blocks at 72 registers measured slower)
 constexpr int kNWr64 = 8, kMinBr64 = 2, kNWr32 = 12, kMinBr32 = 2;
 
-// x-chunk length: fewest estimated block-steps, counting whole waves of the resident slots
-// (ties go to the longer chunk, which recomputes fewer boundary elements)
-static void h8r_launch_dims(const Grid& g, bool fp32, dim3* grid, int* CXc) {
+// Balanced persistent launch: the (tile column, node plane) work of the grid, node planes
+// contiguous within a column, is split evenly over one block per resident slot (at least a
+// few planes per block); a block marches its share in at most a few column segments, each
+// with one boundary element step.  This avoids both the partial last wave and the
+// per-chunk boundary steps of a launch of fixed-length chunks.
+static void h8r_launch_dims(const Grid& g, bool fp32, dim3* grid, H8Tiles* tl) {
     const int ny = g.nn[1], nz = g.nn[2], nx = g.nn[0];
     const int nw = fp32 ? kNWr32 : kNWr64;
-    const int tz = (nz + kZTileR - 1) / kZTileR, ty = (ny + nw - 2) / (nw - 1);
+    const int tz = (nz + kZTileR - 1) / kZTileR;
+    const bool half = nz - (tz - 1) * kZTileR <= kZTileR / 2 - 1;
+    tl->tzA = half ? tz - 1 : tz;
+    tl->tyA = (ny + nw - 2) / (nw - 1);
+    const int tyB = half ? (ny + 2 * nw - 2) / (2 * nw - 1) : 0;
+    tl->ncols = tl->tzA * tl->tyA + tyB;
     const long long slots = (long long)kNumSM * (fp32 ? kMinBr32 : kMinBr64);
-    const long long cols = (long long)tz * ty;
-    int best = 4;
-    long long best_cost = -1;
-    for (int cx = 4; cx <= 64; cx++) {
-        const long long nb = cols * ((nx + cx - 1) / cx);
-        const long long cost = ((nb + slots - 1) / slots) * (cx + 1);
-        if (best_cost < 0 || cost <= best_cost) {
-            best_cost = cost;
-            best = cx;
-        }
-    }
-    *CXc = best;
-    *grid = dim3(tz, ty, (nx + best - 1) / best);
+    const long long total = (long long)tl->ncols * nx;
+    long long nb = (total + 3) / 4;  // at least four node planes per block
+    if (nb > slots) nb = slots;
+    if (nb < 1) nb = 1;
+    *grid = dim3((unsigned)nb, 1, 1);
 }
 
 long long h8_num_blocks(const Grid& g, int fp32) {
     dim3 gr;
-    int cx;
-    h8r_launch_dims(g, fp32 != 0, &gr, &cx);
+    H8Tiles tl;
+    h8r_launch_dims(g, fp32 != 0, &gr, &tl);
     return (long long)gr.x * gr.y * gr.z;
 }
 
@@ -872,19 +899,19 @@ long long q4_num_blocks(const Grid& g) { return (g.n_nodes + 255) / 256; }
 // launchers
 // ---------------------------------------------------------------------------------------
 template <typename T, typename TE, int CM, int MODE, bool DOT>
-static int h8r_launch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
+static int h8r_launch(dim3 grid, H8Tiles tl, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
                       const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, cudaStream_t st) {
     constexpr int MINB = sizeof(T) == 8 ? kMinBr64 : kMinBr32, NW = sizeof(T) == 8 ? kNWr64 : kNWr32;
     PF_CUDA(launch_pdl(k_matvec_h8r<T, TE, NW, MINB, CM, MODE, DOT>, dim3(grid), dim3(NW * 32), 0, st,
-                       g.nel[0], g.nel[1], g.nel[2], cx, u, E, mask, blk, cf, epi));
+                       g.nel[0], g.nel[1], g.nel[2], tl, u, E, mask, blk, cf, epi));
     return PF_OK;
 }
 
 // the epilogue mode and the fused dot are template parameters of the kernel
 template <typename T, typename TE, int CM>
-static int h8r_dispatch(dim3 grid, int cx, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
+static int h8r_dispatch(dim3 grid, H8Tiles tl, const Grid& g, const T* u, const TE* E, const uint8_t* mask,
                         const H8Blk<T>& blk, const H8Coef<T>& cf, const Epi<T>& epi, bool dot, cudaStream_t st) {
-#define PF_H8R(M, D) return h8r_launch<T, TE, CM, M, D>(grid, cx, g, u, E, mask, blk, cf, epi, st)
+#define PF_H8R(M, D) return h8r_launch<T, TE, CM, M, D>(grid, tl, g, u, E, mask, blk, cf, epi, st)
     switch (epi.mode) {
         case PF_EPI_STORE:
             if (dot) PF_H8R(PF_EPI_STORE, true);
@@ -971,17 +998,17 @@ int launch_fine_matvec(const Op* op, const TE* E, const T* u, const uint8_t* mas
         const H8Blk<T> blk = make_blk<T>(op);
         if (epi.mode < PF_EPI_STORE || epi.mode > PF_EPI_JACOBI_ADD) return fail(PF_BAD_ARG, "unknown epilogue mode");
         dim3 grid;
-        int cx;
-        h8r_launch_dims(g, sizeof(T) == 4, &grid, &cx);
+        H8Tiles tl;
+        h8r_launch_dims(g, sizeof(T) == 4, &grid, &tl);
         pf::count_launch();
         const bool dot = epi.dot_partial != nullptr;
         int s;
         if (cm == 2)
-            s = h8r_dispatch<T, TE, 2>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+            s = h8r_dispatch<T, TE, 2>(grid, tl, g, u, E, mask, blk, cf, epi, dot, st);
         else if (cm == 1)
-            s = h8r_dispatch<T, TE, 1>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+            s = h8r_dispatch<T, TE, 1>(grid, tl, g, u, E, mask, blk, cf, epi, dot, st);
         else
-            s = h8r_dispatch<T, TE, 0>(grid, cx, g, u, E, mask, blk, cf, epi, dot, st);
+            s = h8r_dispatch<T, TE, 0>(grid, tl, g, u, E, mask, blk, cf, epi, dot, st);
         if (s) return s;
     } else {
         const long long nb = q4_num_blocks(g);

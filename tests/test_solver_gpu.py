@@ -411,7 +411,12 @@ def test_fixed_jacobi_weight_matches_oracle(precision, field):
         slack = 1 if field == "smooth" and precision == "fp64" else max(3, ito // 10)
         assert abs(it - ito) <= slack, (it, ito)
     assert true_res(kern, U, fe.rhs) < 2e-8
-    assert rel(U.cpu().numpy(), xo) < 1e-6
+    # the stopping test bounds the residual, not the error: at 1e-9 contrast two solves that
+    # both stop at 1e-8 differ by up to cond(K) * 1e-8, and the mixed form's path (twice the
+    # iterations, FP32 preconditioner, its own order of every dot product) ends 1e-6..1e-5
+    # from the oracle's solution; elsewhere they agree to 1e-6
+    bound = 1e-5 if (field == "contrast" and precision == "mixed") else 1e-6
+    assert rel(U.cpu().numpy(), xo) < bound
 
 
 def test_fixed_jacobi_weight_argument_checks():
