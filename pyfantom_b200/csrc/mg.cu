@@ -74,6 +74,7 @@ struct pf_mg {
     int defl = 0;
     float* yf = nullptr;
     double* Wd = nullptr;
+    double* gscratch = nullptr;  // intermediate stencils of the separable Galerkin product (levels >= 2)
     double* dG = nullptr;
     float* Ef = nullptr;            // FP32 element scales of the V-cycle (precision 1)
     __nv_bfloat16* Eb = nullptr;    // BF16 element scales of the V-cycle (precision 2)
@@ -648,7 +649,7 @@ static void mg_free(pf_mg* mg) {
     coarse_destroy(mg->c1);
     mg->c1 = nullptr;
     for (void* p : {(void*)mg->K0_dev, (void*)mg->Kc_dev, (void*)mg->elem_flag, (void*)mg->node_flag, (void*)mg->Ef,
-                    (void*)mg->Eb, (void*)mg->yf, (void*)mg->Wd, (void*)mg->dG,
+                    (void*)mg->Eb, (void*)mg->yf, (void*)mg->Wd, (void*)mg->dG, (void*)mg->gscratch,
                     (void*)mg->r, (void*)mg->p, (void*)mg->q, (void*)mg->partials, (void*)mg->st,
                     (void*)mg->Eint, (void*)mg->bi, (void*)mg->xi})
         if (p) cudaFree(p);
@@ -738,6 +739,12 @@ extern "C" int pf_mg_create(const pf_op* op, const pf_mg_config* cfg, pf_mg** ou
         }
         gl = coarse_grid(gl);
     }
+    long long gsc = 0;
+    for (int l = 2; l <= mg->nlev; l++) {
+        const long long need = galerkin_sep_scratch(mg->L[l - 1].g);
+        if (need > gsc) gsc = need;
+    }
+    if (gsc > 0) s = s ? s : dalloc((void**)&mg->gscratch, (size_t)gsc * sizeof(double));
     const long long ncoarse = mg->L[mg->nlev].ndof;
     if (!s && ncoarse > 6144)
         s = fail(PF_BAD_ARG, "coarsest level has %lld DOF (> 6144): use more levels", ncoarse);
@@ -848,7 +855,7 @@ extern "C" int pf_mg_setup(pf_mg* mg, const double* E, const uint8_t* node_mask,
     if ((s = launch_galerkin_l0(g, E, node_mask, mg->elem_flag, mg->node_flag, mg->K0_dev, mg->Kc_dev, mg->L[1].A64, st)))
         return s;
     for (int l = 2; l <= mg->nlev; l++)
-        if ((s = launch_galerkin_l1p(mg->L[l - 1].g, mg->L[l - 1].A64, mg->L[l].A64, st))) return s;
+        if ((s = launch_galerkin_sep(mg->L[l - 1].g, mg->L[l - 1].A64, mg->L[l].A64, mg->gscratch, st))) return s;
     for (int l = 1; l < mg->nlev; l++) {
         Level& L = mg->L[l];
         const bool half = L.H != nullptr;  // level 1 with the element operator has no stencil copy

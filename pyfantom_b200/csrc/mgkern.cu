@@ -693,6 +693,53 @@ __global__ void __launch_bounds__(128) k_galerkin_l1p(GridDev<DIM> gf, GridDev<D
     for (int a = 0; a < BS; a++) Ac[((long long)(o * BS + a)) * Nc + I] = blk[a];
 }
 
+// One axis of the Galerkin product of a 3D level >= 2.  R = D Phat^T and P = Phat D are
+// tensor products of per-axis factors (linear-interpolation weights 0.5^|d|, the per-axis
+// part 1/1.5 or 1/2 of 1/tw, the bounds of each axis), so A_c = R A P is three one-axis
+// products, x, then y, then z, each on a grid coarsened along the axes already done.  An
+// output entry (node I, offset O) sums over the admissible (dn, dm) pairs of its axis only
+// (at most 7, against up to 343 triples in k_galerkin_l1p): 2197 instead of 5 x 13^3 terms per
+// coarse node summed over its 27 offsets, with the first pass on the fine grid coalesced.  Same
+// operator, other rounding order.
+template <int AX>
+__global__ void __launch_bounds__(128) k_galerkin_axis(GridDev<3> gi, GridDev<3> go, const double* __restrict__ Si,
+                                                       double* __restrict__ So) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long No = go.n_nodes, Ni = gi.n_nodes;
+    if (tid >= No * 27) return;
+    const int o = (int)(tid / No);
+    const long long I = tid - (long long)o * No;
+    int c[3];
+    ndec(go, I, c[0], c[1], c[2]);
+    const int oo[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+    const int Ia = c[AX], Ta = Ia + oo[AX];
+    double blk[9];
+#pragma unroll
+    for (int a = 0; a < 9; a++) blk[a] = 0.0;
+    if (Ta >= 0 && Ta < go.nn[AX]) {
+        const int np = c_npairs[oo[AX] + 1];
+        for (int p = 0; p < np; p++) {
+            const int dn = c_pairs[oo[AX] + 1][p][0], dm = c_pairs[oo[AX] + 1][p][1];
+            const int na = 2 * Ia + dn, ma = 2 * Ta + dm;
+            if (na < 0 || na >= gi.nn[AX] || ma < 0 || ma >= gi.nn[AX]) continue;
+            const double w = (dn != 0 ? 0.5 : 1.0) * (dm != 0 ? 0.5 : 1.0);
+            int ci[3] = {c[0], c[1], c[2]}, ri[3] = {oo[0], oo[1], oo[2]};
+            ci[AX] = na;
+            ri[AX] = ma - na;
+            const long long n = nidx(gi, ci[0], ci[1], ci[2]);
+            const int on = (ri[0] + 1) + 3 * (ri[1] + 1) + 9 * (ri[2] + 1);
+#pragma unroll
+            for (int a = 0; a < 9; a++) blk[a] += w * Si[((long long)(on * 9 + a)) * Ni + n];
+        }
+        const int nn = go.nn[AX];
+        const double s = 1.0 / (((Ia == 0 || Ia == nn - 1) ? 1.5 : 2.0) * ((Ta == 0 || Ta == nn - 1) ? 1.5 : 2.0));
+#pragma unroll
+        for (int a = 0; a < 9; a++) blk[a] *= s;
+    }
+#pragma unroll
+    for (int a = 0; a < 9; a++) So[((long long)(o * 9 + a)) * No + I] = blk[a];
+}
+
 static bool g_pairs_ready = false;
 static int init_pairs() {
     if (g_pairs_ready) return PF_OK;
@@ -725,6 +772,35 @@ int launch_galerkin_l1p(const Grid& gf, const double* Af, double* Ac, cudaStream
     else
         k_galerkin_l1p<2><<<nb, 128, 0, st>>>(gdev<2>(gf), gdev<2>(gc), Af, Ac);
     PF_LAUNCH_CHECK("galerkin l1p launch");
+    return PF_OK;
+}
+
+// the fine grid with one axis coarsened (element count halved, floored)
+static Grid coarsen_axis(const Grid& g, int ax) {
+    int nel[3] = {g.nel[0], g.nel[1], g.nel[2]};
+    nel[ax] /= 2;
+    return make_grid(g.dim, nel);
+}
+
+long long galerkin_sep_scratch(const Grid& gf) {
+    if (gf.dim != 3) return 0;
+    const Grid g1 = coarsen_axis(gf, 0), g2 = coarsen_axis(g1, 1);
+    return 243LL * (g1.n_nodes + g2.n_nodes);
+}
+
+int launch_galerkin_sep(const Grid& gf, const double* Af, double* Ac, double* scratch, cudaStream_t st) {
+    if (gf.dim != 3) return launch_galerkin_l1p(gf, Af, Ac, st);
+    int s = init_pairs();
+    if (s) return s;
+    const Grid g1 = coarsen_axis(gf, 0), g2 = coarsen_axis(g1, 1), gc = coarsen_axis(g2, 2);
+    double* S1 = scratch;
+    double* S2 = scratch + 243LL * g1.n_nodes;
+    auto nb = [](const Grid& g) { return (unsigned)((g.n_nodes * 27 + 127) / 128); };
+    pf::count_launch(3);
+    k_galerkin_axis<0><<<nb(g1), 128, 0, st>>>(gdev<3>(gf), gdev<3>(g1), Af, S1);
+    k_galerkin_axis<1><<<nb(g2), 128, 0, st>>>(gdev<3>(g1), gdev<3>(g2), S1, S2);
+    k_galerkin_axis<2><<<nb(gc), 128, 0, st>>>(gdev<3>(g2), gdev<3>(gc), S2, Ac);
+    PF_LAUNCH_CHECK("separable galerkin launch");
     return PF_OK;
 }
 

@@ -36,6 +36,10 @@ int launch_galerkin_l0(const Grid& gf, const double* E, const uint8_t* mask, con
                        const uint8_t* node_flag, const double* K0_dev, const double* Kc_dev, double* A,
                        cudaStream_t st);
 int launch_galerkin_l1p(const Grid& gf, const double* Af, double* Ac, cudaStream_t st);
+// the same product as three one-axis passes (3D; 2D falls back to launch_galerkin_l1p);
+// scratch holds galerkin_sep_scratch(gf) doubles
+long long galerkin_sep_scratch(const Grid& gf);
+int launch_galerkin_sep(const Grid& gf, const double* Af, double* Ac, double* scratch, cudaStream_t st);
 template <typename T>
 int launch_stencil_dinv(const Grid& g, const double* A, T* dinv, cudaStream_t st);
 int launch_stencil_to_dense(const Grid& g, const double* A, double* M, long long ld, cudaStream_t st);
